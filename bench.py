@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Zone-updates/s of the 3D relativistic jet on B200.
+
+Workload (per GPU): 3D relativistic jet, 512^3 interior cells (+3 ghosts per
+side), Gamma = 4/3, WENOZ + HLLC, SSP-RK3, CFL 0.4 (dt = 0.4 / (3/dx)).
+Ambient rho = 1 with 3% seeded multiplicative noise (as the reference's jet
+example adds, examples/Jet3D/HARM_jet_breakout.jl:91-94), p = 1e-3, v = 0; a
+nozzle of radius 16 cells on the x = 0 face injects rho = 0.01, p = 1e-3,
+Lorentz factor 10 along +x; outflow elsewhere. Synthetic, generated on the
+device. Inputs (5.6 GB of primitives per array) exceed L2 (126 MB).
+
+Headline (`value`): the FP32-bulk form (FP32 reconstruction/flux/divergence,
+FP64 conserved variables and con2prim) with the learned con2prim guess when the
+network is available, else the previous-state guess; reported next to the plain
+FP64 path on the same workload and the L1 rho/p error of the fast path against
+it. `e2e`: the same fast path through the public API with host buffers
+(pinned FP64 AoS primitives in, K steps, primitives out).
+
+--impl reference: the reference has no runnable CPU path here (it is Julia and
+its 2D/3D drivers need CUDA.jl); the oracle's C restatement of the same scheme
+is timed on all host cores on a bounded sub-box of the workload instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s on 1 B200, 3D jet: learned+FP32 vs plain FP64 at fixed L1 error"
+UNIT = "zone-updates/s"
+GAMMA = 4.0 / 3.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=512, help="interior cells per axis")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def workload_config(n, guess):
+    return {
+        "workload": f"3D relativistic jet {n}^3, WENOZ+HLLC, SSP-RK3, CFL 0.4, gamma 4/3, nozzle r=16 Gamma=10",
+        "grid": [n, n, n],
+        "recon": "WENOZ",
+        "riemann": "HLLC",
+        "rk": 3,
+        "precision": "fp32 bulk (fp64 U, RK accumulation, con2prim)",
+        "con2prim_guess": guess,
+        "ic": "ambient rho=1 (3% seeded noise), p=1e-3, v=0; nozzle rho=0.01 p=1e-3 Gamma=10",
+        "l2": "inputs larger than L2 (5.6 GB per primitive array)",
+        "parallelism": "replicas",
+    }
+
+
+# ---- shared problem setup -------------------------------------------------------
+def nozzle(n):
+    import math
+
+    return [16.0, n / 2, n / 2, 0.01, 1e-3 / (GAMMA - 1), math.sqrt(99.0), 0.0, 0.0]
+
+
+def device_ic(n, seed):
+    """Primitive AoS array of the workload on the device (torch, reversed shape)."""
+    import torch
+
+    m = n + 6
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    P = torch.zeros((m, m, m, 5), dtype=torch.float64, device="cuda")
+    P[..., 0] = 1.0 + 0.03 * torch.randn((m, m, m), generator=gen, dtype=torch.float64, device="cuda")
+    P[..., 1] = 1e-3 / (GAMMA - 1)
+    return P
+
+
+def make_solver(n, precision, guess):
+    from verona_b200 import Solver
+
+    dx = 1.0 / n
+    s = Solver(3, (n, n, n), GAMMA, (dx, dx, dx), recon="wenoz", riemann="hllc", rk=3, precision=precision,
+               guess=guess, n_iter=50, tol=1e-12, floor=1e-8)
+    s.set_boundary(0, 2, nozzle(n))
+    return s
+
+
+def dt_of(n):
+    return 0.4 / (3.0 * n)
+
+
+# ---- clocks -----------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is None:
+            self.summary = None
+            return
+        time.sleep(0.25)
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nme, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nme)
+        self.summary = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                        "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---- timing -------------------------------------------------------------------------
+def timed_steps(s, dt, warmup, steps, dist=None):
+    import torch
+
+    stream = torch.cuda.current_stream()
+    s.step(dt, warmup)
+    torch.cuda.synchronize()
+    s.profile(True)
+    s.profile_read()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step(dt, steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    stage_ms, stage_launches, launches = s.profile_read()
+    s.profile(False)
+    return ms, stage_ms, stage_launches, launches
+
+
+def l1_errors(a, b):
+    """L1 relative error of rho and p (interior) of run a against run b."""
+    import torch
+
+    ai, bi = a[3:-3, 3:-3, 3:-3], b[3:-3, 3:-3, 3:-3]
+    out = {}
+    for name, v in (("rho", 0), ("p", 1)):
+        out[name] = float((ai[..., v] - bi[..., v]).abs().mean() / bi[..., v].abs().mean())
+    la = torch.sqrt(1 + (ai[..., 2:] ** 2).sum(-1))
+    lb = torch.sqrt(1 + (bi[..., 2:] ** 2).sum(-1))
+    out["lorentz_max_abs"] = float((la - lb).abs().max())
+    return out
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic(key):
+    """Per-cell DRAM bytes of the stage kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "stage_kernel_traffic.txt")
+    try:
+        for line in open(path):
+            f = line.split()
+            if len(f) >= 2 and f[0] == key:
+                return float(f[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---- CPU baseline (the oracle, test infrastructure, as the checker's timing) -------------
+def cpu_baseline(seconds):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import numpy as np
+
+    from oracle import oracle as O
+
+    S = 96
+    n = (S, S, S)
+    rng = np.random.default_rng(42)
+    P = np.zeros((5, S + 6, S + 6, S + 6), order="F")
+    P[0] = 1.0 + 0.03 * rng.standard_normal(P.shape[1:])
+    P[1] = 1e-3 / (GAMMA - 1)
+    s = O.SolverND(3, n, P, GAMMA, 1e-8, 50, 1e-12, O.WENOZ, O.HLLC, 3)
+    s.set_grid(1.0 / S, 1.0 / S, 1.0 / S)
+    s.set_boundary(0, O.BC_NOZZLE, [16.0 * S / 512 * 4, S / 2, S / 2, 0.01, 3e-3, 99 ** 0.5, 0, 0])
+    dt = dt_of(S)
+    t0 = time.perf_counter()
+    s.step(dt, 1)
+    one = time.perf_counter() - t0
+    k = max(1, int(seconds / max(one, 1e-3)))
+    t0 = time.perf_counter()
+    s.step(dt, k)
+    el = time.perf_counter() - t0
+    return {
+        "value": S**3 * k / el,
+        "unit": UNIT,
+        "cores": O.num_threads(),
+        "kind": "port",
+        "sample": f"oracle (C FP64 restatement, OpenMP) on a {S}^3 sub-box of the same jet workload "
+                  f"(WENOZ+HLLC+RK3, FP64), {k} steps after 1 warm-up step, {el:.1f} s",
+    }
+
+
+# ---- arms ------------------------------------------------------------------------------
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    cb = cpu_baseline(args.cpu_seconds * max(1, args.steps) / 10.0)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args.n, "previous state (reference)"),
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference (Julia/CUDA.jl) does not run here; its scheme is timed as the oracle's C restatement",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+
+    import verona_b200  # noqa: F401  (fails loudly if the CUDA library is missing)
+    from verona_b200 import _lib
+
+    n, K, W = args.n, args.steps, args.warmup
+    dt = dt_of(n)
+    cells = n**3
+    learned_ok = False
+    try:
+        from verona_b200 import mlp  # noqa: F401
+
+        learned_ok = mlp.available()
+    except Exception:
+        learned_ok = False
+    guess = "learned" if learned_ok else "previous"
+    P0 = device_ic(n, 42 + rank)
+    info = {}
+
+    # plain FP64 path (same scheme, reference con2prim)
+    fp64 = None
+    if not args.no_fp64:
+        s = make_solver(n, "fp64", "previous")
+        s.load_prims(P0)
+        ms, st_ms, st_l, ln = timed_steps(s, dt, W, K, dist)
+        fp64 = {"value": cells * K / (ms / 1e3), "ms_per_step": ms / K, "stage_ms_per_launch": st_ms / max(st_l, 1)}
+        P64 = s.store_prims()
+        torch.cuda.synchronize()
+        info["fp64_counters"] = s.counters().tolist()
+        s.close()
+        del s
+
+    # headline: FP32 bulk (+ learned guess when available)
+    s = make_solver(n, "fp32", guess)
+    if learned_ok:
+        mlp.attach(s)
+    s.load_prims(P0)
+    with Clocks(torch.cuda.current_device()) as clk:
+        ms, st_ms, st_l, launches = timed_steps(s, dt, W, K, dist)
+    Pf = s.store_prims()
+    torch.cuda.synchronize()
+    info["fast_counters"] = s.counters().tolist()
+    err = l1_errors(Pf, P64) if fp64 else None
+    del Pf
+
+    t_tensor = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t_tensor, op=dist.ReduceOp.MAX)
+    ms_max = float(t_tensor.item())
+    value = world * cells * K / (ms_max / 1e3)
+
+    # e2e through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(P0.shape, dtype=torch.float64, pin_memory=True)
+        host.copy_(P0)
+        del P0
+        torch.cuda.synchronize()
+        s.load_prims(host.numpy().transpose(3, 2, 1, 0))  # warm the staging buffer
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        s.load_prims(host.numpy().transpose(3, 2, 1, 0))
+        s.step(dt, K)
+        s.prims_into(host.numpy().transpose(3, 2, 1, 0))
+        el = time.perf_counter() - t0
+        tt = torch.tensor([el], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        el = float(tt.item())
+        nbytes = host.numel() * 8
+        e2e = {"value": world * cells * K / el, "unit": UNIT, "h2d_bytes_per_step": nbytes / K,
+               "d2h_bytes_per_step": nbytes / K,
+               "note": f"one H2D of the FP64 AoS primitives, {K} steps, one D2H (the HARM_HLL call pattern)"}
+    s.close()
+
+    if rank != 0:
+        return
+    # roofline of the dominant kernel (the fused stage kernel): algorithmic bytes
+    # per zone-update for FP32-bulk SSP-RK3 = 6*5*4 (P) + 8*5*8 (U) = 440 B
+    peak, peak_kind = read_peaks()
+    bytes_per_cell_step = 440.0
+    stage_ms_per_step = st_ms / K
+    achieved = cells * bytes_per_cell_step / (stage_ms_per_step / 1e3) / 1e9
+    traffic = read_traffic("fp32_wenoz_hllc_rk3")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 bulk + f64 (U, con2prim)", "data": "synthetic",
+        "config": workload_config(n, guess),
+        "fp64_plain": fp64,
+        "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
+        "l1_error_vs_fp64": err,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic * cells / 3 if traffic else None, "peak_kind": peak_kind,
+                     "kernel": "k_stage (fused reconstruct+HLLC+divergence+RK+con2prim)",
+                     "algorithmic_bytes_per_zone_update": bytes_per_cell_step,
+                     "stage_ms_per_launch": st_ms / max(st_l, 1)},
+        "gpu_launches": launches,
+        "clocks": clk.summary,
+        "e2e": e2e,
+        "counters": info,
+    }
+    if not os.environ.get("VB_BENCH_NO_CPU"):
+        line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as D
+
+        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+        dist = D
+    try:
+        run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+/*
+ * verona_b200.h -- C ABI of the B200 SRHD step library (libverona_b200.so).
+ *
+ * Drop-in for the per-timestep update of Wesenheit/Verona's HARM_HLL solvers:
+ *   Verona3D.HARM_HLL   src/3dim/algos.jl:203-362
+ *   Verona2D.HARM_HLL   src/2dim/algos.jl:192-324
+ *   Verona1D.HARM_HLL   src/1dim/algos.jl:169-426
+ * The Julia host keeps grid/state construction, boundary choice, the time
+ * loop and HDF5 output; it hands the library the device pointer of P.arr and
+ * calls vb_step between dumps. Plain pointers, sizes and an opaque handle
+ * only: no C++ or framework types cross this boundary.
+ *
+ * Conventions
+ *  - Every function returns VB_OK (0) or a negative VB_ERR_* code; the text
+ *    of the last error of a handle is returned by vb_last_error(h) (or the
+ *    last global error for h == NULL). No exceptions cross the ABI and no
+ *    device code traps: con2prim failures are counted (vb_get_counters), as
+ *    the reference marks them with NaN (src/3dim/structs.jl:612-619).
+ *  - Primitive arrays at the boundary are the reference's own layout: FP64,
+ *    column-major (nvar, Nx+6, Ny+6[, Nz+6]) with the variable index fastest
+ *    and 3 ghost cells per side (src/3dim/structs.jl:28-64); nvar = 2 + dims,
+ *    P = (rho, u, u^x[, u^y[, u^z]]). The 1D reference layout (nghost = 0)
+ *    is (3, N) with no ghosts (src/1dim/structs.jl:22-34).
+ *  - `stream` is a cudaStream_t (CUDA.jl: stream().handle); NULL is the
+ *    legacy default stream. Work is enqueued on it; only functions that
+ *    return host values or read host buffers synchronise it.
+ *  - A handle belongs to one host thread and one device (the device current
+ *    at vb_create).
+ */
+#ifndef VERONA_B200_H
+#define VERONA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VB_ABI_VERSION 1
+
+enum vb_status_code {
+    VB_OK = 0,
+    VB_ERR_ARG = -1,         /* invalid argument */
+    VB_ERR_CUDA = -2,        /* CUDA runtime error (message in vb_last_error) */
+    VB_ERR_STATE = -3,       /* call not valid in the handle's current state */
+    VB_ERR_UNSUPPORTED = -4, /* option combination not provided */
+    VB_ERR_NOMEM = -5,       /* device allocation failed */
+    VB_ERR_TIMEOUT = -6      /* a bounded device-side wait gave up */
+};
+
+/* reconstruction, src/fluxlimiter.jl:183-200 (`reconstruction(::Val{M})`) */
+enum { VB_RECON_MINMOD = 0, VB_RECON_PPM = 1, VB_RECON_WENOZ = 2 };
+/* Riemann solver: the reference is HLL (src/3dim/algos.jl:149-174); HLLC is an extension */
+enum { VB_RIEMANN_HLL = 0, VB_RIEMANN_HLLC = 1 };
+/* time integrator: 2 = the reference's midpoint RK2 (src/3dim/algos.jl:279-327); 3 = SSP-RK3 */
+enum { VB_RK2 = 2, VB_RK3 = 3 };
+/* precision: FP64 everywhere (reference), or FP32 reconstruction/flux/divergence with
+ * FP64 conserved variables, RK accumulation and con2prim */
+enum { VB_PREC_FP64 = 0, VB_PREC_FP32_BULK = 1 };
+/* con2prim initial guess: the cell's previous primitive state (reference) or the
+ * learned BF16 MLP guess refined by Newton (3D only) */
+enum { VB_GUESS_PREVIOUS = 0, VB_GUESS_LEARNED = 1 };
+/* boundary kinds of vb_set_boundary */
+enum {
+    VB_BC_OUTFLOW = 0, /* zero-gradient copy of the first interior cell (TurnOff's y/z/x-high copies) */
+    VB_BC_FIXED = 1,   /* ghosts keep what was loaded; optional decay {var, t_on, t_off, factor} */
+    VB_BC_NOZZLE = 2   /* {radius, c1, c2, rho, u, u1, u2, u3}: fixed inflow inside, outflow outside */
+};
+enum { VB_FACE_XLO = 0, VB_FACE_XHI = 1, VB_FACE_YLO = 2, VB_FACE_YHI = 3, VB_FACE_ZLO = 4, VB_FACE_ZHI = 5 };
+/* indices of vb_get_counters */
+enum {
+    VB_CNT_C2P_FAIL = 0,     /* cells where con2prim found no root (set to NaN) */
+    VB_CNT_C2P_FALLBACK = 1, /* cells that needed a fallback stage */
+    VB_CNT_C2P_ITERS = 2,    /* Newton iterations (options.stats = 1) */
+    VB_CNT_C2P_CELLS = 3,    /* cells solved (options.stats = 1) */
+    VB_CNT_TIMEOUT = 4,      /* bounded device waits that gave up */
+    VB_CNT_BAD_INDEX = 5,    /* out-of-range work items that were skipped */
+    VB_CNT_N = 8
+};
+
+typedef struct vb_options {
+    uint32_t version;     /* VB_ABI_VERSION */
+    int32_t recon;        /* VB_RECON_*; the 2D/3D reference is WENOZ */
+    int32_t riemann;      /* VB_RIEMANN_* */
+    int32_t rk;           /* VB_RK2 | VB_RK3 */
+    int32_t precision;    /* VB_PREC_* */
+    int32_t guess;        /* VB_GUESS_* */
+    int32_t n_iter;       /* Newton iteration cap: HARM_HLL kwargs[1] (src/3dim/algos.jl:290) */
+    int32_t stats;        /* 1: count Newton iterations (slower) */
+    double tol;           /* Newton tolerance: HARM_HLL kwargs[2] */
+    double floor_;        /* density / internal-energy floor: HARM_HLL `floor` */
+    double w_rtol;        /* learned guess: relative W tolerance of the refinement (1e-12) */
+    int32_t w_max_newton; /* learned guess: Newton steps before the bracketed fallback (8) */
+    int32_t reserved_i[7];
+    double reserved_d[4];
+} vb_options;
+
+typedef struct vb_solver* vb_handle;
+
+/* Fill *o with the reference's defaults (WENOZ, HLL, RK2, FP64, previous-state
+ * guess, n_iter 50, tol 1e-10, floor 1e-7). */
+int vb_default_options(vb_options* o);
+
+/* Create a solver for an nx x ny x nz interior grid (ny = nz = 1 in 1D,
+ * nz = 1 in 2D). nghost = 3 selects the 2D/3D reference semantics and their
+ * ghost-cell layout (src/{2,3}dim/algos.jl; also generic 1D); nghost = 0 with
+ * dims = 1 selects the 1D reference solver on N = nx cells
+ * (src/1dim/algos.jl:169-426). Replaces HARM_HLL's allocations
+ * (src/3dim/algos.jl:221-257). */
+int vb_create(vb_handle* h, int dims, int nx, int ny, int nz, int nghost, const vb_options* o);
+int vb_destroy(vb_handle h);
+const char* vb_last_error(vb_handle h);
+
+/* Polytrope{T}(gamma), src/eos.jl:7-9 */
+int vb_set_eos(vb_handle h, double gamma);
+/* dx, dy, dz of HARM_HLL */
+int vb_set_grid(vb_handle h, double dx, double dy, double dz);
+/* Built-in replacement of the host `fun_bound` callback
+ * (examples/Jet3D/HARM_jet_breakout.jl:131-158): applied on the device at the
+ * start of every step, decay first, then faces y-lo, y-hi, z-lo, z-hi, x-lo,
+ * x-hi. Default: OUTFLOW on every face. */
+int vb_set_boundary(vb_handle h, int face, int kind, const double* params, int nparams);
+
+/* Load P (device, reference layout) and compute U = PtoU(P) on all cells
+ * (kernel_PtoU, src/3dim/structs.jl:66-81; called at src/3dim/algos.jl:259). */
+int vb_load_prims(vb_handle h, const double* P_aos_dev, void* stream);
+/* Write the current P into a device array of the reference layout. */
+int vb_store_prims(vb_handle h, double* P_aos_dev, void* stream);
+/* Host-buffer variants (pinned or pageable); they return after the copy. */
+int vb_load_prims_host(vb_handle h, const double* P_aos_host, void* stream);
+int vb_store_prims_host(vb_handle h, double* P_aos_host, void* stream);
+/* Current conserved state U in the reference layout (device pointer). */
+int vb_store_cons(vb_handle h, double* U_aos_dev, void* stream);
+
+/* Run nsteps iterations of the HARM_HLL time-loop body (src/3dim/algos.jl:274-329):
+ * boundary fill, the RK stages, t += dt. */
+int vb_step(vb_handle h, double dt, int nsteps, void* stream);
+int vb_get_time(vb_handle h, double* t);
+int vb_set_time(vb_handle h, double t);
+
+/* Largest characteristic speed |lambda| over interior cells and axes (HARM
+ * signal speeds of src/3dim/algos.jl:130-157 on cell-centred states); the
+ * CFL dt of an adaptive driver is cfl / sum_d(c / dx_d). Synchronises. */
+int vb_max_signal_speed(vb_handle h, double* c, void* stream);
+
+/* Copy the device counters (VB_CNT_*) into out[0..n). Synchronises. */
+int vb_get_counters(vb_handle h, uint64_t* out, int n, void* stream);
+int vb_reset_counters(vb_handle h, void* stream);
+
+/* Device bytes held by the handle. */
+int vb_memory_bytes(vb_handle h, uint64_t* bytes);
+
+/* Profiling (no counterpart in the reference, which only prints wall-clock
+ * rates, src/3dim/algos.jl:335-353). While enabled, every stage-kernel launch
+ * is bracketed by CUDA events on the caller's stream and every kernel launch
+ * of the library is counted. vb_profile_read synchronises on the last event,
+ * returns the summed stage-kernel time (ms) and the launch counts since the
+ * previous read, and resets them. */
+int vb_profile_enable(vb_handle h, int enable);
+int vb_profile_read(vb_handle h, double* stage_ms, int64_t* stage_launches, int64_t* all_launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VERONA_B200_H */

@@ -526,7 +526,8 @@ static int c2p_3d(double g, int n_iter, double tol, const double* Uc, double* P)
         W = w_small * SQR(gm);
         double W_max = 1e30;
         double W_min = sqrt(S2) * (1.0 + 1e-15);
-        while (S2 / SQR(W) >= 1.0 && W < W_max) W *= 10.0;
+        /* the reference loop never ends for W <= 0; 400 passes cover every positive W */
+        for (int guard = 0; guard < 400 && S2 / SQR(W) >= 1.0 && W < W_max; ++guard) W *= 10.0;
         v2 = jmin(S2 / SQR(W), 1.0 - 1e-15);
         for (int it = 0; it < n_iter; ++it) {
             if (W < W_min) W = W_min;
@@ -561,7 +562,8 @@ static int c2p_3d(double g, int n_iter, double tol, const double* Uc, double* P)
         double w_small = P[0] + g * P[1];
         W = w_small * SQR(gm);
         double W_max = 1e30;
-        while (S2 / SQR(W) >= 1.0 && W < W_max) W *= 10.0;
+        /* the reference loop never ends for W <= 0; 400 passes cover every positive W */
+        for (int guard = 0; guard < 400 && S2 / SQR(W) >= 1.0 && W < W_max; ++guard) W *= 10.0;
         v2 = jmin(S2 / SQR(W), 1.0 - 1e-15);
         double W_old, v2_old;
         for (int it = 0; it < n_iter; ++it) {

@@ -1,0 +1,84 @@
+"""CPU checks of the C ABI: the in-tree library loads and exports every
+function that include/verona_b200.h declares, and argument validation that
+needs no GPU behaves as documented. No compute calls are made here."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")]
+
+
+def declared_functions():
+    names = set()
+    for h in HEADERS:
+        txt = open(h).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(vb\w+)\s*\(", txt, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_the_api():
+    names = declared_functions()
+    for n in ("vb_create", "vb_step", "vb_load_prims", "vb_store_prims", "vb_destroy", "vb_last_error"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    from verona_b200 import _lib
+
+    L = _lib.lib()
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (vb\w+)", out))
+    missing = [n for n in declared_functions() if n not in exported]
+    assert not missing, missing
+    for n in declared_functions():
+        assert getattr(L, n) is not None
+
+
+def test_default_options_are_the_reference_defaults():
+    from verona_b200 import _lib
+
+    o = _lib.default_options()
+    assert o.version == _lib.ABI_VERSION
+    assert (o.recon, o.riemann, o.rk, o.precision, o.guess) == (2, 0, 2, 0, 0)
+    assert o.n_iter == 50 and o.tol == 1e-10 and o.floor_ == 1e-7
+
+
+@pytest.mark.parametrize(
+    "args,needle",
+    [
+        ((4, 8, 8, 8, 3), "dims"),
+        ((2, 0, 8, 1, 3), "interior size"),
+        ((2, 8, 8, 1, 0), "nghost"),
+        ((3, 8, 8, 8, 2), "nghost"),
+    ],
+)
+def test_create_rejects_bad_arguments_without_a_gpu(args, needle):
+    from verona_b200 import _lib
+
+    h = C.c_void_p()
+    o = _lib.default_options()
+    rc = _lib.lib().vb_create(C.byref(h), *args, C.byref(o))
+    assert rc == _lib.ERR_ARG
+    assert needle in _lib.lib().vb_last_error(None).decode()
+    assert not h.value
+
+
+def test_create_rejects_bad_options_without_a_gpu():
+    from verona_b200 import _lib
+
+    L = _lib.lib()
+    h = C.c_void_p()
+    for kw, code in (({"rk": 4}, _lib.ERR_ARG), ({"recon": 7}, _lib.ERR_ARG), ({"n_iter": 0}, _lib.ERR_ARG),
+                     ({"guess": 1}, _lib.ERR_UNSUPPORTED)):
+        o = _lib.default_options(**kw)
+        assert L.vb_create(C.byref(h), 2, 8, 8, 1, 3, C.byref(o)) == code, kw
+    o = _lib.default_options()
+    o.version = 99
+    assert L.vb_create(C.byref(h), 2, 8, 8, 1, 3, C.byref(o)) == _lib.ERR_ARG
+    assert L.vb_step(None, 0.1, 1, None) == _lib.ERR_ARG

@@ -1,0 +1,253 @@
+"""GPU parity tests: the CUDA path, called through the C ABI, against the CPU
+oracle on the same seeded inputs.
+
+Bar: the plain FP64 path matches the oracle to a max relative difference of
+1e-10 per conserved field (normalised by the field's max magnitude) after
+the stated step count; with -fmad=false it is expected to be bit-identical
+and the tests also report how many values differ at all.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from helpers import jet_ic, n_steps, nozzle_params, per_field_rel, shock_tube_1d
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL = 1e-10  # FP64 parity bar per conserved field
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(os.path.join(GOLDEN, "oracle_small.npz"))
+
+
+@pytest.fixture(scope="module")
+def MG():
+    sys.path.insert(0, GOLDEN)
+    import make_golden
+
+    return make_golden
+
+
+def _solver_nd(dims, n, P, gamma, dxs, **opt):
+    from verona_b200 import Solver
+
+    s = Solver(dims, n[:dims], gamma, dxs, **opt)
+    return s
+
+
+@pytest.mark.parametrize("rec", ["minmod", "ppm", "wenoz"])
+def test_ref1d_matches_golden_bitwise(gold, MG, rec):
+    from verona_b200 import Solver
+
+    for r, N, steps in MG.CASES_1D:
+        if r != rec:
+            continue
+        g = 5.0 / 3.0
+        x, rho, u, ux = shock_tube_1d(N, gamma=g)
+        s = Solver(1, (N,), g, (1.0 / N,), nghost=0, recon=rec, n_iter=50, tol=1e-12)
+        s.load_prims(np.asfortranarray(np.stack([rho, u, ux])))
+        s.step(0.4 / N, steps)
+        P = s.prims()
+        np.testing.assert_array_equal(P, gold[f"r1d_{rec}_P"])
+        np.testing.assert_array_equal(s.cons(), gold[f"r1d_{rec}_U"])
+
+
+@pytest.mark.parametrize("rec", ["minmod", "ppm", "wenoz"])
+def test_ref1d_shock_tube_full_run_matches_oracle(oracle, rec):
+    """Config 1: N = 1024, t = 0.4, CFL 0.4, through the Verona1D mirror."""
+    from verona_b200 import EosTypes, Verona1D
+
+    g = 5.0 / 3.0
+    N = 1024
+    x, rho, u, ux = shock_tube_1d(N, gamma=g)
+    dx = 1.0 / N
+    dt = 0.4 * dx
+    P = Verona1D.ParVector1D(N, rho, u, ux)
+    out = Verona1D.HARM_HLL(P, N, dt, dx, 0.4, EosTypes.Polytrope(g), 0.4 / 3, rec, 50, 1e-12)
+    assert len(out) == 4  # t = 0 plus three dumps
+    s = oracle.Solver1DRef(rho, u, ux, g, rec, 50, 1e-12)
+    n, _ = n_steps(dt, 0.4)
+    s.step(dt, dx, n)
+    ref = s.prims()
+    got = np.stack([P.arr1, P.arr2, P.arr3])
+    assert max(per_field_rel(got, ref)) <= TOL
+    print(f"{rec}: {int(np.sum(got != ref))} of {got.size} values differ from the oracle")
+
+
+def test_nd_matches_golden(gold, MG):
+    from verona_b200 import Solver
+
+    for c in MG.CASES_ND:
+        dims, n, rec, rs, rk, steps = c
+        g = 4.0 / 3.0
+        P0 = jet_ic(dims, n, gamma=g, noise=0.03, seed=7)
+        dxs = [1.0 / n[a] for a in range(dims)]
+        s = Solver(dims, n[:dims], g, dxs, recon=rec, riemann=rs, rk=rk, n_iter=50, tol=1e-12, floor=1e-8)
+        s.set_boundary(0, 2, nozzle_params(dims, n, 3.0, gamma=g))
+        s.load_prims(P0)
+        dt = 0.4 / sum(1.0 / d for d in dxs)
+        s.step(dt, steps)
+        name = MG.nd_case_name(c)
+        P, U = s.prims(), s.cons()
+        eP = per_field_rel(P, gold[name + "_P"])
+        eU = per_field_rel(U, gold[name + "_U"])
+        print(name, "max rel P", max(eP), "U", max(eU), "differing:", int(np.sum(P != gold[name + "_P"])))
+        assert max(eU) <= TOL and max(eP) <= TOL, (name, eP, eU)
+
+
+@pytest.mark.parametrize("dims,n,steps", [(2, (64, 48, 1), 20), (3, (24, 20, 18), 8)])
+@pytest.mark.parametrize("rk", [2, 3])
+def test_jet_parity_with_decaying_inflow(oracle, dims, n, steps, rk):
+    """A reference-style jet (WENOZ + HLL) with the TurnOff boundary: x-lo fixed
+    with a u^x decay that switches on mid-run, zero-gradient elsewhere."""
+    from verona_b200 import Solver
+
+    g = 4.0 / 3.0
+    P0 = jet_ic(dims, n, gamma=g, noise=0.03, seed=11)
+    # jet state in the x-lo ghosts inside r < 4 cells
+    yy = np.arange(n[1] + 6) - 3 + 0.5 - n[1] / 2
+    zz = (np.arange(n[2] + 6) - 3 + 0.5 - n[2] / 2) if dims == 3 else np.zeros(1)
+    Y, Z = np.meshgrid(yy, zz, indexing="ij")
+    inside = (Y**2 + Z**2) < 16.0
+    m = inside if dims == 3 else inside[:, 0]
+    for i in range(3):
+        for v, val in ((0, 0.01), (1, 3e-3), (2, np.sqrt(99.0))):
+            P0[v, i][m] = val
+    dxs = [1.0 / n[0]] * dims
+    dt = 0.4 / sum(1.0 / d for d in dxs)
+    decay = (2, 3.5 * dt, 1e9, 1 - dt / 0.05)
+    s = Solver(dims, n[:dims], g, dxs, recon="wenoz", riemann="hll", rk=rk, n_iter=50, tol=1e-12, floor=1e-8)
+    s.set_boundary(0, 1, decay)
+    s.load_prims(P0)
+    s.step(dt, steps)
+    o = oracle.SolverND(dims, n[:dims], P0, g, 1e-8, 50, 1e-12, oracle.WENOZ, oracle.HLL, rk)
+    o.set_grid(*(dxs + [1.0] * (3 - dims)))
+    o.set_boundary(0, oracle.BC_FIXED, decay)
+    o.step(dt, steps)
+    eU = per_field_rel(s.cons(), o.cons())
+    eP = per_field_rel(s.prims(), o.prims())
+    print(dims, rk, "U", eU, "P", eP)
+    assert max(eU) <= TOL and max(eP) <= TOL
+
+
+def test_fp32_bulk_close_to_fp64():
+    from verona_b200 import Solver
+
+    g = 4.0 / 3.0
+    n = (32, 24, 24)
+    P0 = jet_ic(3, n, gamma=g, noise=0.03, seed=5)
+    dxs = [1.0 / 32] * 3
+    dt = 0.4 / sum(1.0 / d for d in dxs)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        s = Solver(3, n, g, dxs, recon="wenoz", riemann="hllc", rk=3, precision=prec, n_iter=50, tol=1e-12,
+                   floor=1e-8)
+        s.set_boundary(0, 2, nozzle_params(3, n, 4.0, gamma=g))
+        s.load_prims(P0)
+        s.step(dt, 10)
+        out[prec] = s.prims()
+        assert s.counters()[0] == 0
+    a, b = out["fp32"][:, 3:-3, 3:-3, 3:-3], out["fp64"][:, 3:-3, 3:-3, 3:-3]
+    l1_rho = np.mean(np.abs(a[0] - b[0])) / np.mean(np.abs(b[0]))
+    l1_p = np.mean(np.abs(a[1] - b[1])) / np.mean(np.abs(b[1]))
+    print("fp32 bulk: L1 rho", l1_rho, "L1 p", l1_p)
+    assert l1_rho < 1e-5 and l1_p < 1e-5
+
+
+def test_max_signal_speed_matches_numpy():
+    from verona_b200 import Solver
+
+    g = 4.0 / 3.0
+    n = (20, 18, 16)
+    rng = np.random.default_rng(2)
+    P0 = jet_ic(3, n, gamma=g, noise=0.2, seed=2)
+    P0[2:] = rng.uniform(-3, 3, size=P0[2:].shape)
+    s = Solver(3, n, g, (0.1, 0.1, 0.1))
+    s.load_prims(P0)
+    c = s.max_signal_speed()
+    Q = P0[:, 3:-3, 3:-3, 3:-3]
+    lor = np.sqrt(Q[2] ** 2 + Q[3] ** 2 + Q[4] ** 2 + 1)
+    cs = np.sqrt(g * (g - 1) * Q[1] / (Q[0] + g * Q[1]))
+    sig = cs**2 / (lor**2 * (1 - cs**2))
+    best = 0.0
+    for d in range(3):
+        v = Q[2 + d] / lor
+        r = np.sqrt(sig * (1 - v**2 + sig))
+        best = max(best, np.max(np.abs((v + r) / (1 + sig))), np.max(np.abs((v - r) / (1 + sig))))
+    assert abs(c - best) <= 1e-14 * best
+
+
+def test_host_and_device_loads_agree():
+    import torch
+
+    from verona_b200 import Solver
+
+    g = 4.0 / 3.0
+    n = (16, 12)
+    P0 = jet_ic(2, n + (1,), gamma=g, seed=9)
+    a = Solver(2, n, g, (0.1, 0.1))
+    a.load_prims(P0)
+    b = Solver(2, n, g, (0.1, 0.1))
+    b.load_prims(torch.from_numpy(np.ascontiguousarray(P0.transpose(2, 1, 0))).cuda())
+    a.step(0.01, 3)
+    b.step(0.01, 3)
+    np.testing.assert_array_equal(a.prims(), b.prims())
+    d = b.store_prims()
+    np.testing.assert_array_equal(d.cpu().numpy().transpose(2, 1, 0), a.prims())
+
+
+def test_reference_mirror_3d_harm_hll(oracle):
+    """Verona3D.HARM_HLL with the TurnOff-equivalent boundary, against the oracle."""
+    from verona_b200 import EosTypes, Verona3D
+
+    g = 4.0 / 3.0
+    n = (16, 12, 12)
+    P0 = jet_ic(3, n, gamma=g, seed=13)
+    P0[2, :3, 4:10, 4:10] = 3.0
+    P = Verona3D.ParVector3D(*n)
+    P.arr[:] = P0
+    dx = 0.05
+    dt = 0.4 / (3 / dx)
+    Tmax, drops = 12 * dt, 4 * dt
+    bnd = Verona3D.turnoff_boundary(dt, 0.1, 9 * dt)
+    dumps = []
+    i = Verona3D.HARM_HLL(None, P, (1, 1, 1), (4, 4, 4), dt, dx, dx, dx, Tmax, EosTypes.Polytrope(g), drops, 1e-8,
+                          ".", False, 50, 1e-12, bnd, dump=lambda k, t, s: dumps.append(k))
+    assert i == len(dumps) - 1 and i >= 2
+    o = oracle.SolverND(3, n, P0, g, 1e-8, 50, 1e-12, oracle.WENOZ, oracle.HLL, 2)
+    o.set_grid(dx, dx, dx)
+    for face, kind, par in bnd:
+        o.set_boundary(face, kind, par)
+    steps, _ = n_steps(dt, Tmax)
+    o.step(dt, steps)
+    assert max(per_field_rel(P.arr, o.prims())) <= TOL
+
+
+def test_healthy_run_has_no_failures_and_counts_iterations():
+    from verona_b200 import Solver
+
+    g = 4.0 / 3.0
+    n = (24, 16, 16)
+    s = Solver(3, n, g, (0.05,) * 3, stats=1, n_iter=50, tol=1e-12, floor=1e-8)
+    s.set_boundary(0, 2, nozzle_params(3, n, 3.0, gamma=g))
+    s.load_prims(jet_ic(3, n, gamma=g))
+    s.step(0.005, 4)
+    c = s.counters()
+    assert c[0] == 0
+    assert c[3] == 2 * 4 * 24 * 16 * 16  # cells solved: 2 stages x 4 steps
+    assert c[2] >= c[3]
+
+
+def test_errors_are_reported_not_trapped():
+    from verona_b200 import Solver, VBError
+
+    s = Solver(2, (8, 8), 4.0 / 3.0, (0.1, 0.1))
+    with pytest.raises(VBError, match="vb_load_prims first"):
+        s.step(0.01, 1)
+    with pytest.raises(VBError, match="face"):
+        s.set_boundary(5, 0)

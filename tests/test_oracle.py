@@ -1,0 +1,152 @@
+"""CPU tests that pin the oracle (the C restatement of the reference) before
+it is trusted as the parity checker of the GPU path.
+
+The reference ships no tests or golden vectors and cannot run here (Julia),
+so the pins are: the published exact solution of Marti & Mueller problem 1,
+the self-convergence idea of examples/Shock1Dim/Resolution_comp.jl,
+uniform-state preservation, mirror symmetry, conservation, the P->U->P round
+trip, and the committed oracle fixtures of tests/golden/.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from helpers import jet_ic, n_steps, nozzle_params, shock_tube_1d
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_exact_solver_matches_published_star_state():
+    from oracle import exact_riemann as ER
+
+    with open(os.path.join(GOLDEN, "mm1_star.json")) as f:
+        star = json.load(f)
+    ps, vs, rl, rr, sl, sr = ER.star_state(10.0, 13.33, 0.0, 1.0, 1e-6, 0.0, 5.0 / 3.0)
+    got = {"p_star": ps, "v_star": vs, "rho_L_star": rl, "rho_R_star": rr, "shock_R": sr}
+    for k, pub in star["published"].items():
+        # the published values carry 3-4 significant digits
+        assert abs(got[k] - pub) <= 6e-4 * max(1.0, abs(pub)), (k, got[k], pub)
+        assert abs(got[k] - star["exact"][k]) <= 1e-9 * abs(star["exact"][k]), k
+
+
+@pytest.mark.parametrize("rec", ["minmod", "ppm", "wenoz"])
+def test_oracle_1d_converges_to_exact_solution(oracle, rec):
+    from oracle import exact_riemann as ER
+
+    g = 5.0 / 3.0
+    errs = []
+    for N in (128, 256, 512):
+        x, rho, u, ux = shock_tube_1d(N, gamma=g)
+        s = oracle.Solver1DRef(rho, u, ux, g, rec, 50, 1e-12)
+        dx = 1.0 / N
+        dt = 0.4 * dx
+        n, t = n_steps(dt, 0.4)
+        s.step(dt, dx, n)
+        P = s.prims()
+        assert np.all(np.isfinite(P))
+        ex = ER.solve(10.0, 13.33, 0.0, 1.0, 1e-6, 0.0, g, x, t)
+        errs.append(float(np.mean(np.abs(P[0] - ex[0]))))
+    assert errs[0] > errs[1] > errs[2], errs
+    assert errs[2] < 0.06, errs
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_oracle_uniform_state_is_preserved(oracle, dims):
+    n = (10, 8, 6)[:dims]
+    g = 4.0 / 3.0
+    P = jet_ic(dims, n + (1,) * (3 - dims), gamma=g, noise=0.0)
+    P[2] = 0.3  # uniform drift
+    for rec in (oracle.MINMOD, oracle.PPM, oracle.WENOZ):
+        for rs in (oracle.HLL, oracle.HLLC):
+            s = oracle.SolverND(dims, n, P, g, 1e-8, 50, 1e-12, rec, rs, 2)
+            s.set_grid(0.1, 0.1, 0.1)
+            s.step(0.01, 3)
+            Q = s.prims()
+            assert np.max(np.abs(Q - P)) <= 1e-12 * np.max(np.abs(P)), (rec, rs)
+
+
+def test_oracle_2d_mirror_symmetry(oracle):
+    n = (16, 16)
+    g = 4.0 / 3.0
+    P = jet_ic(2, n + (1,), gamma=g, noise=0.03, seed=3)
+    P[:] = 0.5 * (P + P[:, :, ::-1])  # symmetric in y
+    P[3] = 0.0
+    s = oracle.SolverND(2, n, P, g, 1e-8, 50, 1e-12, oracle.WENOZ, oracle.HLL, 2)
+    s.set_grid(1 / 16, 1 / 16)
+    s.set_boundary(0, oracle.BC_NOZZLE, nozzle_params(2, (16, 16, 1), 3.0, gamma=g))
+    s.step(0.4 / 32, 5)
+    Q = s.prims()
+    M = Q[:, :, ::-1].copy()
+    M[3] = -M[3]
+    assert np.max(np.abs(Q - M)) <= 1e-12 * np.max(np.abs(Q))
+
+
+@pytest.mark.parametrize("rs", ["hll", "hllc"])
+def test_oracle_conservation(oracle, rs):
+    """Outflow box whose edges stay at the same ambient state: the fluxes
+    through opposite faces cancel, so sum(U) over the interior is conserved."""
+    n = (24, 24)
+    g = 4.0 / 3.0
+    P = jet_ic(2, n + (1,), gamma=g, noise=0.0)
+    xi, yj = np.meshgrid(np.arange(30) - 14.5, np.arange(30) - 14.5, indexing="ij")
+    P[0] += 0.5 * np.exp(-(xi**2 + yj**2) / 8.0)
+    rsv = oracle.HLL if rs == "hll" else oracle.HLLC
+    s = oracle.SolverND(2, n, P, g, 1e-8, 50, 1e-12, oracle.WENOZ, rsv, 3)
+    s.set_grid(1.0, 1.0)
+    U0 = s.cons()[:, 3:-3, 3:-3].sum(axis=(1, 2))
+    s.step(0.2, 4)
+    U1 = s.cons()[:, 3:-3, 3:-3].sum(axis=(1, 2))
+    for v in range(4):
+        scale = max(abs(U0[0]), abs(U0[1]))
+        assert abs(U1[v] - U0[v]) <= 1e-12 * scale, (v, U0[v], U1[v])
+
+
+def test_oracle_con2prim_round_trip(oracle):
+    rng = np.random.default_rng(1)
+    for dims in (1, 2, 3):
+        for _ in range(300):
+            g = rng.choice([4.0 / 3.0, 5.0 / 3.0])
+            rho = 10 ** rng.uniform(-4, 1)
+            p = rho * 10 ** rng.uniform(-6, 2)
+            lor = 10 ** rng.uniform(0, np.log10(40.0 if dims == 3 else 10.0))
+            d = rng.normal(size=dims)
+            d /= np.linalg.norm(d)
+            uvec = np.sqrt(lor**2 - 1) * d
+            if dims == 3 and (rho / lor < 1e-6 or p / (g - 1) < 1e-6):
+                continue  # the 3D solver floors rho and u at 1e-8 by design (src/3dim/structs.jl:602-603)
+            P = np.concatenate([[rho, p / (g - 1)], uvec])
+            U = oracle.prim2con(dims, g, P)
+            guess = P * (1 + 1e-3 * rng.standard_normal(P.shape))
+            Q, r = oracle.con2prim(dims, g, 200, 1e-13, U, guess)
+            assert r >= 1, (dims, P, r)
+            # compare through the conserved state (primitive u is ill-conditioned when p << rho)
+            assert np.max(np.abs(oracle.prim2con(dims, g, Q) - U)) <= 1e-9 * np.max(np.abs(U)), (dims, P, Q)
+
+
+def test_oracle_reproduces_golden_fixtures(oracle):
+    import sys
+
+    sys.path.insert(0, GOLDEN)
+    import make_golden as MG
+
+    gold = np.load(os.path.join(GOLDEN, "oracle_small.npz"))
+    for rec, N, steps in MG.CASES_1D:
+        _, P, U, _, _ = MG.run_1d_case(rec, N, steps)
+        np.testing.assert_array_equal(P, gold[f"r1d_{rec}_P"])
+        np.testing.assert_array_equal(U, gold[f"r1d_{rec}_U"])
+    for c in MG.CASES_ND:
+        _, P, U, _, _ = MG.run_nd_case(c)
+        name = MG.nd_case_name(c)
+        np.testing.assert_array_equal(P, gold[name + "_P"])
+        np.testing.assert_array_equal(U, gold[name + "_U"])
+
+
+def test_oracle_3d_con2prim_floors_like_the_reference(oracle):
+    """u below 1e-8 comes back floored at 1e-8 (src/3dim/structs.jl:603)."""
+    g = 4.0 / 3.0
+    P = np.array([1e-3, 1e-10, 0.5, 0.1, -0.2])
+    U = oracle.prim2con(3, g, P)
+    Q, r = oracle.con2prim(3, g, 50, 1e-12, U, P)
+    assert r >= 1 and Q[1] == 1e-8

@@ -1,0 +1,123 @@
+"""ctypes binding of libverona_b200.so (include/verona_b200.h).
+
+The library is built in-tree (verona_b200/build.py). Loading fails loudly if
+it is missing: there is no CPU fallback of any kind.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libverona_b200.so")
+
+ABI_VERSION = 1
+OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_UNSUPPORTED, ERR_NOMEM, ERR_TIMEOUT = 0, -1, -2, -3, -4, -5, -6
+RECON = {"minmod": 0, "ppm": 1, "wenoz": 2, "MINMOD": 0, "PPM": 1, "WENOZ": 2}
+RIEMANN = {"hll": 0, "hllc": 1, "HLL": 0, "HLLC": 1}
+PRECISION = {"fp64": 0, "fp32": 1, "fp32_bulk": 1}
+GUESS = {"previous": 0, "learned": 1}
+BC_OUTFLOW, BC_FIXED, BC_NOZZLE = 0, 1, 2
+FACE = {"xlo": 0, "xhi": 1, "ylo": 2, "yhi": 3, "zlo": 4, "zhi": 5}
+CNT_C2P_FAIL, CNT_C2P_FALLBACK, CNT_C2P_ITERS, CNT_C2P_CELLS, CNT_TIMEOUT, CNT_BAD_INDEX = range(6)
+CNT_N = 8
+
+
+class VBOptions(C.Structure):
+    _fields_ = [
+        ("version", C.c_uint32),
+        ("recon", C.c_int32),
+        ("riemann", C.c_int32),
+        ("rk", C.c_int32),
+        ("precision", C.c_int32),
+        ("guess", C.c_int32),
+        ("n_iter", C.c_int32),
+        ("stats", C.c_int32),
+        ("tol", C.c_double),
+        ("floor_", C.c_double),
+        ("w_rtol", C.c_double),
+        ("w_max_newton", C.c_int32),
+        ("reserved_i", C.c_int32 * 7),
+        ("reserved_d", C.c_double * 4),
+    ]
+
+
+class VBError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"verona_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+_vp = C.c_void_p
+_dp = C.POINTER(C.c_double)
+
+# name -> (argtypes); every function returns int
+_SIGS = {
+    "vb_default_options": [C.POINTER(VBOptions)],
+    "vb_create": [C.POINTER(_vp), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(VBOptions)],
+    "vb_destroy": [_vp],
+    "vb_set_eos": [_vp, C.c_double],
+    "vb_set_grid": [_vp, C.c_double, C.c_double, C.c_double],
+    "vb_set_boundary": [_vp, C.c_int, C.c_int, _dp, C.c_int],
+    "vb_load_prims": [_vp, _vp, _vp],
+    "vb_store_prims": [_vp, _vp, _vp],
+    "vb_load_prims_host": [_vp, _vp, _vp],
+    "vb_store_prims_host": [_vp, _vp, _vp],
+    "vb_store_cons": [_vp, _vp, _vp],
+    "vb_step": [_vp, C.c_double, C.c_int, _vp],
+    "vb_get_time": [_vp, _dp],
+    "vb_set_time": [_vp, C.c_double],
+    "vb_max_signal_speed": [_vp, _dp, _vp],
+    "vb_get_counters": [_vp, C.POINTER(C.c_uint64), C.c_int, _vp],
+    "vb_reset_counters": [_vp, _vp],
+    "vb_memory_bytes": [_vp, C.POINTER(C.c_uint64)],
+    "vb_profile_enable": [_vp, C.c_int],
+    "vb_profile_read": [_vp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
+}
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def lib():
+    """Load the in-tree library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m verona_b200.build` (no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.vb_last_error.argtypes = [_vp]
+        L.vb_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def check(rc: int, handle=None):
+    if rc != OK:
+        msg = lib().vb_last_error(handle)
+        raise VBError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def default_options(**kw) -> VBOptions:
+    o = VBOptions()
+    check(lib().vb_default_options(C.byref(o)))
+    for k, v in kw.items():
+        if k == "recon" and isinstance(v, str):
+            v = RECON[v]
+        elif k == "riemann" and isinstance(v, str):
+            v = RIEMANN[v]
+        elif k == "precision" and isinstance(v, str):
+            v = PRECISION[v]
+        elif k == "guess" and isinstance(v, str):
+            v = GUESS[v]
+        elif k == "floor":
+            k = "floor_"
+        setattr(o, k, v)
+    return o

@@ -1,0 +1,477 @@
+// Conservative-to-primitive recovery ("con2prim"), FP64, one cell per thread.
+//
+// c2p_1d / c2p_2d / c2p_3d restate the reference's three per-dimension
+// algorithms in the reference's own evaluation order; c2p_w is the
+// guess-driven 1D Newton on W = rho h gamma^2 with a bracketed fallback used
+// by the learned-guess path. Every loop is bounded by n_iter (or a fixed cap);
+// nothing here spins, traps or asserts -- failures are returned as codes.
+#pragma once
+#include "vb_physics.cuh"
+
+namespace vb {
+
+VB_HD double vb_nan() { return NAN; }
+
+// 3x3 solve of the 1D Newton (src/1dim/structs.jl:94; StaticArrays `\`):
+// adjugate formula with the determinant as a column triple product.
+VB_HD void solve3(const double* A, const double* b, double* x) {
+#define a(r, c) A[((r)-1) + 3 * ((c)-1)]
+    double c1 = a(2, 2) * a(3, 3) - a(3, 2) * a(2, 3);
+    double c2 = a(3, 2) * a(1, 3) - a(1, 2) * a(3, 3);
+    double c3 = a(1, 2) * a(2, 3) - a(2, 2) * a(1, 3);
+    double det = a(1, 1) * c1 + a(2, 1) * c2 + a(3, 1) * c3;
+    x[0] = ((a(2, 2) * a(3, 3) - a(2, 3) * a(3, 2)) * b[0] + (a(1, 3) * a(3, 2) - a(1, 2) * a(3, 3)) * b[1] +
+            (a(1, 2) * a(2, 3) - a(1, 3) * a(2, 2)) * b[2]) / det;
+    x[1] = ((a(2, 3) * a(3, 1) - a(2, 1) * a(3, 3)) * b[0] + (a(1, 1) * a(3, 3) - a(1, 3) * a(3, 1)) * b[1] +
+            (a(1, 3) * a(2, 1) - a(1, 1) * a(2, 3)) * b[2]) / det;
+    x[2] = ((a(2, 1) * a(3, 2) - a(2, 2) * a(3, 1)) * b[0] + (a(1, 2) * a(3, 1) - a(1, 1) * a(3, 2)) * b[1] +
+            (a(1, 1) * a(2, 2) - a(1, 2) * a(2, 1)) * b[2]) / det;
+#undef a
+}
+
+// 1D UtoP, src/1dim/structs.jl:78-105 (F_ptoU :48-54, Jacobian :32-46).
+// The stop rule drops the last delta. Returns the iteration count.
+VB_HD int c2p_1d(double g, int n_iter, double tol, const double* U, double* P) {
+    double x1 = P[0], x2 = P[1], x3 = P[2];
+    int it;
+    for (it = 1; it <= n_iter; ++it) {
+        double gam = sqrt(sq(x3) + 1.0);
+        double w = g * x2 + x1;
+        double f[3], J[9], dl[3];
+        f[0] = gam * x1;
+        f[1] = (g - 1.0) * x2 - sq(gam) * w;
+        f[2] = x3 * gam * w;
+        double gj = sqrt(1.0 + sq(x3));
+        double wj = g * x2 + x1;
+        J[0] = gj;
+        J[3] = 0.0;
+        J[6] = x1 * x3 / gj;
+        J[1] = -sq(gj);
+        J[4] = (g - 1.0) - sq(gj) * g;
+        J[7] = -2.0 * x3 * wj;
+        J[2] = gj * x3;
+        J[5] = gj * x3 * g;
+        J[8] = (2.0 * sq(x3) + 1.0) / gj * wj;
+        f[0] = f[0] - U[0];
+        f[1] = f[1] - U[1];
+        f[2] = f[2] - U[2];
+        solve3(J, f, dl);
+        if (sqrt(sq(dl[0]) + sq(dl[1]) + sq(dl[2])) < tol) break;
+        x1 = x1 - dl[0];
+        x2 = x2 - dl[1];
+        x3 = x3 - dl[2];
+    }
+    P[0] = x1;
+    P[1] = x2;
+    P[2] = x3;
+    return it;
+}
+
+// LU_dec_pivot!, src/2dim/structs.jl:121-208. Returns false on a row-wise
+// singular matrix (the reference raises an error there).
+VB_HD bool lu_pivot4(double* A, double* t, double* x) {
+#define I4(i, j) (((j)-1) * 4 + (i)-1)
+    double rn[4];
+    for (int i = 1; i <= 4; ++i) {
+        double am = 0.0;
+        for (int j = 1; j <= 4; ++j) {
+            double tmp = fabs(A[I4(i, j)]);
+            if (tmp > am) am = tmp;
+        }
+        if (am == 0.0) return false;
+        rn[i - 1] = 1.0 / am;
+    }
+    for (int k = 1; k <= 4; ++k) {
+        int piv = k;
+        double pv = fabs(A[I4(k, k)]) * rn[k - 1];
+        for (int i = k + 1; i <= 4; ++i) {
+            double tmp = fabs(A[I4(i, k)]) * rn[i - 1];
+            if (tmp > pv) {
+                pv = tmp;
+                piv = i;
+            }
+        }
+        if (piv != k) {
+            for (int j = 1; j <= 4; ++j) {
+                double tmp = A[I4(k, j)];
+                A[I4(k, j)] = A[I4(piv, j)];
+                A[I4(piv, j)] = tmp;
+            }
+            double tmp = t[k - 1];
+            t[k - 1] = t[piv - 1];
+            t[piv - 1] = tmp;
+            tmp = rn[k - 1];
+            rn[k - 1] = rn[piv - 1];
+            rn[piv - 1] = tmp;
+        }
+        for (int i = k + 1; i <= 4; ++i) {
+            A[I4(i, k)] /= A[I4(k, k)];
+            for (int j = k + 1; j <= 4; ++j) A[I4(i, j)] = fma(-A[I4(i, k)], A[I4(k, j)], A[I4(i, j)]);
+        }
+    }
+    for (int i = 1; i <= 4; ++i) {
+        x[i - 1] = t[i - 1];
+        for (int j = 1; j <= i - 1; ++j) x[i - 1] = fma(-A[I4(i, j)], x[j - 1], x[i - 1]);
+    }
+    for (int i = 4; i >= 1; --i) {
+        for (int j = i + 1; j <= 4; ++j) x[i - 1] = fma(-A[I4(i, j)], x[j - 1], x[i - 1]);
+        x[i - 1] /= A[I4(i, i)];
+    }
+#undef I4
+    return true;
+}
+
+// 2D function_UtoP, src/2dim/structs.jl:249-330. Returns the iteration count,
+// -1 on a singular Jacobian.
+VB_HD int c2p_2d(double g, int n_iter, double tol, const double* U, double* P) {
+    int it;
+    for (it = 1; it <= n_iter; ++it) {
+        double gam = sqrt(sq(P[2]) + sq(P[3]) + 1.0);
+        double w = g * P[1] + P[0];
+        double f[4], J[16], o[4];
+        f[0] = gam * P[0] - U[0];
+        f[1] = (g - 1.0) * P[1] - sq(gam) * w - U[1];
+        f[2] = P[2] * gam * w - U[2];
+        f[3] = P[3] * gam * w - U[3];
+        J[0] = gam;
+        J[4] = 0.0;
+        J[8] = P[0] * P[2] / gam;
+        J[12] = P[0] * P[3] / gam;
+        J[1] = -sq(gam);
+        J[5] = (g - 1.0) - sq(gam) * g;
+        J[9] = -2.0 * P[2] * w;
+        J[13] = -2.0 * P[3] * w;
+        J[2] = gam * P[2];
+        J[6] = gam * P[2] * g;
+        J[10] = (2.0 * sq(P[2]) + sq(P[3]) + 1.0) / gam * w;
+        J[14] = P[2] * P[3] / gam * w;
+        J[3] = gam * P[3];
+        J[7] = gam * P[3] * g;
+        J[11] = P[2] * P[3] / gam * w;
+        J[15] = (2.0 * sq(P[3]) + sq(P[2]) + 1.0) / gam * w;
+        if (!lu_pivot4(J, f, o)) return -1;
+        if (sqrt(sq(o[0]) + sq(o[1]) + sq(o[2]) + sq(o[3])) < tol) break;
+        P[0] = P[0] - o[0];
+        P[1] = P[1] - o[1];
+        P[2] = P[2] - o[2];
+        P[3] = P[3] - o[3];
+    }
+    return it;
+}
+
+// LU_dec_5D! / LU_dec_2D!, src/3dim/structs.jl:144-214 (no pivoting)
+template <int N> VB_HD void lu_plain(double* A, const double* t, double* x) {
+#define IX(i, j) (((j)-1) * N + (i)-1)
+    for (int k = 1; k <= N; ++k)
+        for (int i = k + 1; i <= N; ++i) {
+            A[IX(i, k)] /= A[IX(k, k)];
+            for (int j = k + 1; j <= N; ++j) A[IX(i, j)] -= A[IX(i, k)] * A[IX(k, j)];
+        }
+    for (int i = 1; i <= N; ++i) {
+        x[i - 1] = t[i - 1];
+        for (int j = 1; j <= i - 1; ++j) x[i - 1] -= A[IX(i, j)] * x[j - 1];
+    }
+    for (int i = N; i >= 1; --i) {
+        for (int j = i + 1; j <= N; ++j) x[i - 1] -= A[IX(i, j)] * x[j - 1];
+        x[i - 1] /= A[IX(i, i)];
+    }
+#undef IX
+}
+
+// Final primitive state from a converged W (src/3dim/structs.jl:598-609).
+VB_HD void prims_from_W(double g, double D, double Qx, double Qy, double Qz, double S2, double W,
+                        double* P) {
+    double v2 = S2 / sq(W);
+    double gm = 1.0 / sqrt(1.0 - v2);
+    gm = jmin(gm, 50.0);
+    double rho = jmax(1e-8, D / gm);
+    double UU = jmax(1e-8, (W / sq(gm) - D / gm) / g);
+    P[0] = rho;
+    P[1] = UU;
+    P[2] = gm * Qx / W;
+    P[3] = gm * Qy / W;
+    P[4] = gm * Qz / W;
+}
+
+// 3D function_UtoP, src/3dim/structs.jl:258-620: 1DW Newton -> Noble 2D
+// Newton with line search -> 5x5 primitive Newton -> bisection. Returns the
+// stage that converged (1..4) or -1 (cell set to NaN, as the reference does).
+VB_HD int c2p_3d(double g, int n_iter, double tol, const double* Uc, double* P) {
+    const double D = Uc[0], Q_t = Uc[1], Q_x = Uc[2], Q_y = Uc[3], Q_z = Uc[4];
+    bool conv1 = false, conv2 = false, conv5 = false, convb = false;
+    double S2, W, v2;
+    {
+        S2 = Q_x * Q_x + Q_y * Q_y + Q_z * Q_z;
+        double gm = sqrt(sq(P[2]) + sq(P[3]) + sq(P[4]) + 1.0);
+        double w_small = P[0] + g * P[1];
+        W = w_small * sq(gm);
+        const double W_max = 1e30;
+        double W_min = sqrt(S2) * (1.0 + 1e-15);
+        for (int guard = 0; guard < 400 && S2 / sq(W) >= 1.0 && W < W_max; ++guard) W *= 10.0;
+        v2 = jmin(S2 / sq(W), 1.0 - 1e-15);
+        for (int it = 0; it < n_iter; ++it) {
+            if (W < W_min) W = W_min;
+            v2 = S2 / sq(W);
+            if (v2 < 0.0)
+                v2 = 0.0;
+            else if (v2 > 1.0 - 1e-15)
+                v2 = 1.0 - 1e-15;
+            double k = (g - 1.0) / g;
+            double bf = Q_t + W - k * (W * (1.0 - v2) - D * sqrt(1.0 - v2));
+            double W3 = W * W * W;
+            double bj = 1.0 - ((g - 1.0) / g) * (1.0 - v2) -
+                        ((g - 1.0) / g) * (W * (2.0 * S2 / W3) - D * (S2 / (W3 * sqrt(1.0 - v2))));
+            double dW = bf / bj;
+            double Wp = W - dW;
+            if (Wp < W_min)
+                W = 0.5 * (W + W_min);
+            else
+                W = Wp;
+            if (dW < 0) dW = -dW;
+            if (sq(dW) < sq(tol)) {
+                conv1 = true;
+                break;
+            }
+        }
+    }
+    if (!conv1) {
+        S2 = Q_x * Q_x + Q_y * Q_y + Q_z * Q_z;
+        double gm = sqrt(sq(P[2]) + sq(P[3]) + sq(P[4]) + 1.0);
+        double w_small = P[0] + g * P[1];
+        W = w_small * sq(gm);
+        const double W_max = 1e30;
+        for (int guard = 0; guard < 400 && S2 / sq(W) >= 1.0 && W < W_max; ++guard) W *= 10.0;
+        v2 = jmin(S2 / sq(W), 1.0 - 1e-15);
+        for (int it = 0; it < n_iter; ++it) {
+            double W_old = W, v2_old = v2;
+            double k = (g - 1.0) / g;
+            double f[2], J[4], o[2];
+            f[0] = v2 - S2 / sq(W);
+            f[1] = Q_t + W - k * (W * (1.0 - v2) - D * sqrt(1.0 - v2));
+            J[0] = 2.0 * S2 / (W * W * W);
+            J[1] = 1.0 - k * (1.0 - v2);
+            J[2] = 1.0;
+            J[3] = k * (W - D / (2.0 * sqrt(1.0 - v2)));
+            lu_plain<2>(J, f, o);
+            double dW = o[0], dv2 = o[1];
+            double alpha = 1.0;
+            bool ok = false;
+            for (int ls = 0; ls < 10; ++ls) {
+                double s = sqrt(W - alpha * dW);
+                double Wc = sq(s);
+                double v2c = v2 - alpha * dv2;
+                if (Wc <= 0 || Wc > W_max) Wc = W_old;
+                if (v2c < 0)
+                    v2c = 0.0;
+                else if (v2c >= 1)
+                    v2c = 1.0 - 1e-15;
+                double r1 = v2c - S2 / sq(Wc);
+                double r2 = Q_t + Wc - k * (Wc * (1.0 - v2c) - D * sqrt(1.0 - v2c));
+                double errc = sq(r1) + sq(r2);
+                double r1o = v2 - S2 / sq(W);
+                double r2o = Q_t + W - k * (W * (1.0 - v2) - D * sqrt(1.0 - v2));
+                double erro = sq(r1o) + sq(r2o);
+                if (errc <= erro) {
+                    W = Wc;
+                    v2 = v2c;
+                    ok = true;
+                    break;
+                } else {
+                    alpha *= 0.5;
+                }
+            }
+            if (!ok) {
+                W = W_old;
+                v2 = v2_old;
+            }
+            double relW = sqrt(sq(W - W_old)) / jmax(fabs(W_old), sq(tol));
+            double relv2 = sqrt(sq(v2 - v2_old)) / jmax(fabs(v2_old), sq(tol));
+            if (relW + relv2 < tol) {
+                conv2 = true;
+                break;
+            }
+        }
+    }
+    if (!conv1 && !conv2) {
+        for (int it = 0; it < n_iter; ++it) {
+            double gam = sqrt(sq(P[2]) + sq(P[3]) + sq(P[4]) + 1.0);
+            double w = g * P[1] + P[0];
+            double f[5], J[25], o[5];
+            f[0] = gam * P[0] - Uc[0];
+            f[1] = (g - 1.0) * P[1] - sq(gam) * w - Uc[1];
+            f[2] = P[2] * gam * w - Uc[2];
+            f[3] = P[3] * gam * w - Uc[3];
+            f[4] = P[4] * gam * w - Uc[4];
+            J[0] = gam;
+            J[5] = 0.0;
+            J[10] = P[2] * P[0] / gam;
+            J[15] = P[3] * P[0] / gam;
+            J[20] = P[4] * P[0] / gam;
+            J[1] = -sq(gam);
+            J[6] = g * (-sq(gam)) + g - 1.0;
+            J[11] = -2.0 * P[2] * w;
+            J[16] = -2.0 * P[3] * w;
+            J[21] = -2.0 * P[4] * w;
+            J[2] = P[2] * gam;
+            J[7] = g * P[2] * gam;
+            J[12] = sq(P[2]) * w / gam + w * gam;
+            J[17] = P[2] * P[3] * w / gam;
+            J[22] = P[2] * P[4] * w / gam;
+            J[3] = P[3] * gam;
+            J[8] = g * P[3] * gam;
+            J[13] = P[2] * P[3] * w / gam;
+            J[18] = sq(P[3]) * w / gam + w * gam;
+            J[23] = P[3] * P[4] * w / gam;
+            J[4] = P[4] * gam;
+            J[9] = g * P[4] * gam;
+            J[14] = P[2] * P[4] * w / gam;
+            J[19] = P[3] * P[4] * w / gam;
+            J[24] = sq(P[4]) * w / gam + w * gam;
+            lu_plain<5>(J, f, o);
+            if (sq(o[0]) + sq(o[1]) + sq(o[2]) + sq(o[3]) + sq(o[4]) < sq(tol)) {
+                if (isfinite(P[0]) && isfinite(P[1]) && isfinite(P[2]) && isfinite(P[3]) && isfinite(P[4])) {
+                    conv5 = true;
+                    P[0] = jmax(1e-8, P[0]);
+                    P[1] = jmax(1e-8, P[1]);
+                    double gm = sqrt(sq(P[2]) + sq(P[3]) + sq(P[4]) + 1.0);
+                    P[2] = P[2] / gm;
+                    P[3] = P[3] / gm;
+                    P[4] = P[4] / gm;
+                    gm = jmin(gm, 50.0);
+                    P[2] = P[2] * gm;
+                    P[3] = P[3] * gm;
+                    P[4] = P[4] * gm;
+                }
+                break;
+            }
+            P[0] = P[0] - o[0];
+            P[1] = P[1] - o[1];
+            P[2] = P[2] - o[2];
+            P[3] = P[3] - o[3];
+            P[4] = P[4] - o[4];
+        }
+    }
+    if (!conv1 && !conv2 && !conv5) {
+        S2 = Q_x * Q_x + Q_y * Q_y + Q_z * Q_z;
+        double k = (g - 1.0) / g;
+        double W_min = jmax(1e-15, sqrt(S2));
+        double W_max = W_min * 10.0;
+#define RES(Wv) (Q_t + (Wv) - k * ((Wv) * (1.0 - S2 / sq(Wv)) - D * sqrt(jmax(0.0, 1.0 - S2 / sq(Wv)))))
+        double fmin_ = RES(W_min);
+        double fmax_ = RES(W_max);
+        int count = 0;
+        while (fmin_ * fmax_ > 0 && count < 100) {
+            W_max *= 10.0;
+            fmax_ = RES(W_max);
+            count += 1;
+        }
+        if (fmin_ * fmax_ <= 0) {
+            for (int it = 0; it < n_iter * 10; ++it) {
+                double Wm = 0.5 * (W_min + W_max);
+                double fm = RES(Wm);
+                if (sq(fm) < sq(1e-6)) {
+                    convb = true;
+                    W = Wm;
+                    break;
+                }
+                if (fmin_ * fm < 0) {
+                    W_max = Wm;
+                    fmax_ = fm;
+                } else {
+                    W_min = Wm;
+                    fmin_ = fm;
+                }
+                W = Wm;
+            }
+        }
+#undef RES
+    }
+    if (conv1 || conv2 || convb) prims_from_W(g, D, Q_x, Q_y, Q_z, S2, W, P);
+    if (!conv1 && !conv2 && !conv5 && !convb) {
+        for (int v = 0; v < 5; ++v) P[v] = vb_nan();
+        return -1;
+    }
+    return conv1 ? 1 : conv2 ? 2 : conv5 ? 3 : 4;
+}
+
+// ---- guess-driven W Newton with a bracketed fallback -------------------------
+// Residual of the 1DW scheme (Noble et al. 2006) written in W alone:
+// f(W) = Q_t + W - k (W (1 - v^2) - D sqrt(1 - v^2)), v^2 = S^2 / W^2.
+struct WRes {
+    double f, df;
+};
+VB_HD WRes w_residual(double g, double D, double Q_t, double S2, double W) {
+    double k = (g - 1.0) / g;
+    double v2 = S2 / (W * W);
+    if (v2 > 1.0 - 1e-15) v2 = 1.0 - 1e-15;
+    double s = sqrt(1.0 - v2);
+    WRes r;
+    r.f = Q_t + W - k * (W * (1.0 - v2) - D * s);
+    double W3 = W * W * W;
+    r.df = 1.0 - k * (1.0 - v2) - k * (W * (2.0 * S2 / W3) - D * (S2 / (W3 * s)));
+    return r;
+}
+
+// Newton on W from a guess, to |dW| <= rtol * W, at most max_newton steps;
+// then a safeguarded (bracketed) Newton from the physical bracket
+// [sqrt(S^2)(1+1e-15), W_hi]. Writes the primitive state through the
+// reference's final-state formula and floors. Returns total iterations, or
+// -(iterations) if both failed (cell set to NaN). *used_fallback is set when
+// the bracketed phase ran.
+VB_HD int c2p_w(double g, const double* Uc, double W0, double rtol, int max_newton, int max_bracket,
+                double* P, int* used_fallback) {
+    const double D = Uc[0], Q_t = Uc[1];
+    const double Qx = Uc[2], Qy = Uc[3], Qz = Uc[4];
+    const double S2 = Qx * Qx + Qy * Qy + Qz * Qz;
+    const double Wlo0 = sqrt(S2) * (1.0 + 1e-15);
+    double W = W0;
+    int it = 0;
+    *used_fallback = 0;
+    if (!(W > Wlo0) || !isfinite(W)) W = fmax(Wlo0 * 1.0000001, D - Q_t);
+    for (; it < max_newton; ++it) {
+        WRes r = w_residual(g, D, Q_t, S2, W);
+        double dW = r.f / r.df;
+        double Wn = W - dW;
+        if (!(Wn > Wlo0)) Wn = 0.5 * (W + Wlo0);
+        bool done = fabs(Wn - W) <= rtol * fabs(Wn);
+        W = Wn;
+        if (done && isfinite(W)) {
+            prims_from_W(g, D, Qx, Qy, Qz, S2, W, P);
+            return it + 1;
+        }
+    }
+    // Bracketed Newton: f(Wlo) <= 0 for a physical state; grow Whi until f > 0.
+    *used_fallback = 1;
+    double lo = Wlo0, hi = fmax(2.0 * Wlo0, D - Q_t + 1.0);
+    WRes rl = w_residual(g, D, Q_t, S2, lo);
+    WRes rh = w_residual(g, D, Q_t, S2, hi);
+    for (int k = 0; k < 200 && rh.f * rl.f > 0.0; ++k) {
+        hi *= 4.0;
+        rh = w_residual(g, D, Q_t, S2, hi);
+    }
+    if (!(rh.f * rl.f <= 0.0)) {
+        for (int v = 0; v < 5; ++v) P[v] = vb_nan();
+        return -(it + 1);
+    }
+    W = (W > lo && W < hi) ? W : 0.5 * (lo + hi);
+    for (int k = 0; k < max_bracket; ++k, ++it) {
+        WRes r = w_residual(g, D, Q_t, S2, W);
+        if ((r.f < 0.0) == (rl.f < 0.0)) {
+            lo = W;
+            rl = r;
+        } else {
+            hi = W;
+        }
+        double Wn = W - r.f / r.df;
+        if (!(Wn > lo && Wn < hi)) Wn = 0.5 * (lo + hi);
+        if (fabs(Wn - W) <= rtol * fabs(Wn) || (hi - lo) <= rtol * hi) {
+            prims_from_W(g, D, Qx, Qy, Qz, S2, Wn, P);
+            return it + 1;
+        }
+        W = Wn;
+    }
+    for (int v = 0; v < 5; ++v) P[v] = vb_nan();
+    return -(it + 1);
+}
+
+}  // namespace vb

@@ -1,0 +1,90 @@
+// Internal interfaces between the kernel translation units and the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace vb {
+
+constexpr int NG = 3;  // ghost cells per side, as the reference's ParVector2D/3D
+
+// Device counters written by the kernels (all uint64).
+enum Counter {
+    CNT_C2P_FAIL = 0,      // con2prim found no root (cell set to NaN, as the reference does)
+    CNT_C2P_FALLBACK = 1,  // a later stage of the cascade / the bracketed phase was needed
+    CNT_C2P_ITERS = 2,     // Newton iterations (statistics mode only)
+    CNT_C2P_CELLS = 3,     // cells solved (statistics mode only)
+    CNT_TIMEOUT = 4,       // a bounded wait in a persistent kernel gave up
+    CNT_BAD_INDEX = 5,     // a work item outside its bounds was skipped
+    CNT_N = 8
+};
+
+// Con2prim strategy inside a stage.
+enum { C2P_REFERENCE = 0, C2P_GUESS_W = 1 };
+
+struct StageParams {
+    int n[3];            // padded extents (unused axes = 1)
+    long long sy, sz;    // strides of j and k in cells
+    long long vs;        // stride between variables in elements
+    double dtdx[3];      // dt_stage / dx_d
+    double rk_a, rk_b;   // Uo = rk_a U0 + rk_b (Us - sum dtdx dF); rk_a == 0 -> Uo = Us - ...
+    double gamma, floor_, tol;
+    int n_iter;
+    int c2p_mode;        // C2P_*
+    int stats;           // 1: accumulate iteration statistics
+    double w_rtol;       // C2P_GUESS_W: relative tolerance of the W Newton
+    int w_max_newton;    // C2P_GUESS_W: Newton steps before the bracketed fallback
+    const float* w_guess;  // C2P_GUESS_W: per-cell W guesses (nullptr: derive from Pin)
+    unsigned long long* counters;
+};
+
+template <typename R> struct StageBufs {
+    const R* Pin;
+    R* Pout;
+    const double* U0;
+    const double* Us;
+    double* Uo;
+};
+
+struct Grid {
+    int dims, nv;
+    int n[3];   // padded extents
+    long long sy, sz, vs;
+};
+
+// ---- launchers, explicitly instantiated for R = double (vb_stage_f64.cu) and
+// R = float (vb_stage_f32.cu) --------------------------------------------------
+template <typename R>
+cudaError_t launch_stage(int dims, int rec, int rs, const StageParams& p, const StageBufs<R>& b,
+                         cudaStream_t s);
+// AoS (Julia column-major, variable fastest) FP64 -> internal SoA R; also U0 = PtoU(P) in FP64
+template <typename R>
+cudaError_t launch_load_prims(const Grid& g, const double* P_aos, R* P, double* U0, double gamma,
+                              cudaStream_t s);
+template <typename R>
+cudaError_t launch_store_prims(const Grid& g, const R* P, double* P_aos, cudaStream_t s);
+// ghost cells of Pout = limit(ghost cells of Pin)
+template <typename R>
+cudaError_t launch_ghost_limit(const Grid& g, const R* Pin, R* Pout, double floor_, cudaStream_t s);
+// boundary fill of one face (kind: 0 outflow, 2 nozzle); decay of a FIXED face
+template <typename R>
+cudaError_t launch_bc_face(const Grid& g, R* P, int face, int kind, const double* par, cudaStream_t s);
+template <typename R>
+cudaError_t launch_bc_decay(const Grid& g, R* P, int face, int var, double factor, cudaStream_t s);
+// per-block maxima of the CFL signal speed into partial[], then one block reduces them to out
+template <typename R>
+cudaError_t launch_max_speed(const Grid& g, const R* P, double gamma, double* partial, int max_partial,
+                             double* out, cudaStream_t s);
+
+// 1D reference solver (src/1dim/algos.jl:169-426), FP64, one persistent CTA.
+struct Ref1DState {
+    int N;
+    double *P, *Ph, *U, *Uh, *PL, *PR, *F;  // [3][N] each
+};
+cudaError_t launch_ref1d_init(const Ref1DState& st, const double* P_aos, double gamma, cudaStream_t s);
+cudaError_t launch_ref1d_steps(const Ref1DState& st, double gamma, int rec, int n_iter, double tol,
+                               double dt, double dx, int nsteps, cudaStream_t s);
+cudaError_t launch_ref1d_store(const Ref1DState& st, double* P_aos, cudaStream_t s);
+
+int max_speed_blocks(const Grid& g);
+
+}  // namespace vb

@@ -1,0 +1,346 @@
+// Point physics of the SRHD update, templated on the arithmetic type.
+//
+// Each function follows Wesenheit/Verona's Julia source (file:line cited) in
+// the same evaluation order: a + b + c is (a + b) + c, x^2 is x*x, x^3 is
+// x*x*x, min/max propagate NaN, and only the explicit fma() calls of
+// src/2dim/structs.jl:192,205,212 are fused. The FP64 translation unit is
+// compiled with -fmad=false, so for T = double every result is bit-identical
+// to the reference's rounding (IEEE +,-,*,/,sqrt are correctly rounded on
+// sm_100a). The FP32 unit uses the same code with FP32 constants.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#define VB_HD __host__ __device__ __forceinline__
+
+namespace vb {
+
+enum { REC_MINMOD = 0, REC_PPM = 1, REC_WENOZ = 2 };
+enum { RS_HLL = 0, RS_HLLC = 1 };
+
+template <typename T> VB_HD T sq(T x) { return x * x; }
+
+// Base.max / Base.min for IEEE floats: NaN-propagating, +0 > -0.
+template <typename T> VB_HD T jmax(T x, T y) {
+    T d = x - y;
+    if (isnan(x) || isnan(y)) return d;
+    return signbit(d) ? y : x;
+}
+template <typename T> VB_HD T jmin(T x, T y) {
+    T d = x - y;
+    if (isnan(x) || isnan(y)) return d;
+    return signbit(d) ? x : y;
+}
+// Base.sign: +-1, keeps signed zero, NaN stays NaN.
+template <typename T> VB_HD T jsign(T x) { return x > T(0) ? T(1) : (x < T(0) ? T(-1) : x); }
+
+// ---- reconstruction (src/fluxlimiter.jl) -----------------------------------
+// Every limiter returns (qr_i, ql_ip1): the value of cell i at its left face
+// i-1/2 and at its right face i+1/2.
+
+// MINMOD, src/fluxlimiter.jl:1-13
+template <typename T> VB_HD void minmod(T qm1, T q, T qp1, T& qr, T& ql) {
+    T sp = qp1 - q;
+    T sm = q - qm1;
+    T ssp = jsign(sp), ssm = jsign(sm);
+    T asp = fabs(sp), asm_ = fabs(sm);
+    T dU = T(0.25) * (ssp + ssm) * jmin(asp, asm_);
+    qr = q - dU;
+    ql = q + dU;
+}
+
+// WENO-Z epsilon. The reference's 1e-42 is subnormal in FP32 and would
+// overflow tau/eps; the FP32 form uses a normal epsilon and caps the
+// smoothness indicator (a documented precision-policy choice).
+template <typename T> struct WenoEps;
+template <> struct WenoEps<double> {
+    static VB_HD double eps() { return 1.0e-42; }
+    static VB_HD double cap(double x) { return x; }
+};
+template <> struct WenoEps<float> {
+    static VB_HD float eps() { return 1.0e-30f; }
+    static VB_HD float cap(float x) { return fminf(x, 1.0e15f); }
+};
+
+// WENOZ, src/fluxlimiter.jl:19-71
+template <typename T>
+VB_HD void wenoz(T q_im2, T q_im1, T q_i, T q_ip1, T q_ip2, T& qr_i, T& ql_ip1) {
+    const T c1 = T(13.0) / T(12.0), c2 = T(0.25);
+    T b1 = c1 * sq(q_im2 + q_i - T(2) * q_im1) + c2 * sq(q_im2 + T(3) * q_i - T(4) * q_im1);
+    T b2 = c1 * sq(q_im1 + q_ip1 - T(2) * q_i) + c2 * sq(q_im1 - q_ip1);
+    T b3 = c1 * sq(q_ip2 + q_i - T(2) * q_ip1) + c2 * sq(q_ip2 + T(3) * q_i - T(4) * q_ip1);
+    const T epsL = WenoEps<T>::eps();
+    T tau5 = fabs(b1 - b3);
+    T i1 = WenoEps<T>::cap(tau5 / (b1 + epsL));
+    T i2 = WenoEps<T>::cap(tau5 / (b2 + epsL));
+    T i3 = WenoEps<T>::cap(tau5 / (b3 + epsL));
+
+    T f1 = T(2) * q_im2 - T(7) * q_im1 + T(11) * q_i;
+    T f2 = -q_im1 + T(5) * q_i + T(2) * q_ip1;
+    T f3 = T(2) * q_i + T(5) * q_ip1 - q_ip2;
+    T a1 = T(0.1) * (T(1) + sq(i1)), a2 = T(0.6) * (T(1) + sq(i2)), a3 = T(0.3) * (T(1) + sq(i3));
+    T asum = T(6) * (a1 + a2 + a3);
+    ql_ip1 = (f1 * a1 + f2 * a2 + f3 * a3) / asum;
+
+    f1 = T(2) * q_ip2 - T(7) * q_ip1 + T(11) * q_i;
+    f2 = -q_ip1 + T(5) * q_i + T(2) * q_im1;
+    f3 = T(2) * q_i + T(5) * q_im1 - q_im2;
+    a1 = T(0.1) * (T(1) + sq(i3));
+    a2 = T(0.6) * (T(1) + sq(i2));
+    a3 = T(0.3) * (T(1) + sq(i1));
+    asum = T(6) * (a1 + a2 + a3);
+    qr_i = (f1 * a1 + f2 * a2 + f3 * a3) / asum;
+}
+
+// PPM, src/fluxlimiter.jl:74-180
+template <typename T>
+VB_HD void ppm(T q_im2, T q_im1, T q_i, T q_ip1, T q_ip2, T& qr_out, T& ql_out) {
+    const T C2 = T(1.25);
+    T qa = q_i - q_im1;
+    T qb = q_ip1 - q_i;
+    T dd_im1 = T(0.5) * qa + T(0.5) * (q_im1 - q_im2);
+    T dd = T(0.5) * qb + T(0.5) * qa;
+    T dd_ip1 = T(0.5) * (q_ip2 - q_ip1) + T(0.5) * qb;
+
+    T dph = T(0.5) * (q_im1 + q_i) + (dd_im1 - dd) / T(6);
+    T dph_ip1 = T(0.5) * (q_i + q_ip1) + (dd - dd_ip1) / T(6);
+
+    T d2qc_im1 = q_im2 + q_i - T(2) * q_im1;
+    T d2qc = q_im1 + q_ip1 - T(2) * q_i;
+    T d2qc_ip1 = q_i + q_ip2 - T(2) * q_ip1;
+
+    T qa_tmp = dph - q_im1;
+    T qb_tmp = q_i - dph;
+    qa = T(3) * (q_im1 + q_i - T(2) * dph);
+    qb = d2qc_im1;
+    T qc = d2qc;
+    T qd = T(0);
+    if (jsign(qa) == jsign(qb) && jsign(qa) == jsign(qc))
+        qd = jsign(qa) * jmin(C2 * fabs(qb), jmin(C2 * fabs(qc), fabs(qa)));
+    T dph_tmp = T(0.5) * (q_im1 + q_i) - qd / T(6);
+    if (qa_tmp * qb_tmp < T(0)) dph = dph_tmp;
+
+    qa_tmp = dph_ip1 - q_i;
+    qb_tmp = q_ip1 - dph_ip1;
+    qa = T(3) * (q_i + q_ip1 - T(2) * dph_ip1);
+    qb = d2qc;
+    qc = d2qc_ip1;
+    qd = T(0);
+    if (jsign(qa) == jsign(qb) && jsign(qa) == jsign(qc))
+        qd = jsign(qa) * jmin(C2 * fabs(qb), jmin(C2 * fabs(qc), fabs(qa)));
+    T dphip1_tmp = T(0.5) * (q_i + q_ip1) - qd / T(6);
+    if (qa_tmp * qb_tmp < T(0)) dph_ip1 = dphip1_tmp;
+
+    T d2qf = T(6) * (dph + dph_ip1 - T(2) * q_i);
+    T qr_i = dph;
+    T ql_ip1 = dph_ip1;
+    T dqf_minus = q_i - qr_i;
+    T dqf_plus = ql_ip1 - q_i;
+
+    qa_tmp = dqf_minus * dqf_plus;
+    qb_tmp = (q_ip1 - q_i) * (q_i - q_im1);
+    qa = d2qc_im1;
+    qb = d2qc;
+    qc = d2qc_ip1;
+    qd = d2qf;
+    T qe = T(0);
+    if (jsign(qa) == jsign(qb) && jsign(qa) == jsign(qc) && jsign(qa) == jsign(qd))
+        qe = jsign(qd) * jmin(jmin(C2 * fabs(qa), C2 * fabs(qb)), jmin(C2 * fabs(qc), fabs(qd)));
+
+    qa = jmax(T(fabs(q_im1)), T(fabs(q_im2)));
+    qb = jmax(jmax(T(fabs(q_i)), T(fabs(q_ip1))), T(fabs(q_ip2)));
+    T rho = T(0);
+    if (fabs(qd) > T(1.0e-12) * jmax(qa, qb)) rho = qe / qd;
+
+    T tmp_m = q_i - rho * dqf_minus;
+    T tmp_p = q_i + rho * dqf_plus;
+    T tmp2_m = q_i - T(2) * dqf_plus;
+    T tmp2_p = q_i + T(2) * dqf_minus;
+    if (qa_tmp <= T(0) || qb_tmp <= T(0)) {
+        if (rho <= T(1) - T(1.0e-12)) {
+            qr_i = tmp_m;
+            ql_ip1 = tmp_p;
+        }
+    } else {
+        if (fabs(dqf_minus) >= T(2) * fabs(dqf_plus)) qr_i = tmp2_m;
+        if (fabs(dqf_plus) >= T(2) * fabs(dqf_minus)) ql_ip1 = tmp2_p;
+    }
+    qr_out = qr_i;
+    ql_out = ql_ip1;
+}
+
+// reconstruction(::Val{M}, ...), src/fluxlimiter.jl:183-200
+template <int REC, typename T>
+VB_HD void recon(T q_im2, T q_im1, T q_i, T q_ip1, T q_ip2, T& qr, T& ql) {
+    if (REC == REC_MINMOD)
+        minmod(q_im1, q_i, q_ip1, qr, ql);
+    else if (REC == REC_PPM)
+        ppm(q_im2, q_im1, q_i, q_ip1, q_ip2, qr, ql);
+    else
+        wenoz(q_im2, q_im1, q_i, q_ip1, q_ip2, qr, ql);
+}
+
+// ---- EOS and state conversions ---------------------------------------------
+// SoundSpeed, src/eos.jl:15-21
+template <typename T> VB_HD T sound_speed(T rho, T u, T g) {
+    return sqrt((g * (g - T(1)) * u) / (rho + g * u));
+}
+
+// gam = sqrt(ux^2 + uy^2 + uz^2 + 1), src/3dim/structs.jl:89
+template <int DIM, typename T> VB_HD T lorentz(const T* P) {
+    T s = sq(P[2]);
+    if (DIM > 1) s = s + sq(P[3]);
+    if (DIM > 2) s = s + sq(P[4]);
+    return sqrt(s + T(1));
+}
+
+// function_PtoU, src/3dim/structs.jl:84-96 (2D: src/2dim/structs.jl:87-98)
+template <int DIM, typename T> VB_HD void prim2con(T g, const T* P, T* U) {
+    T gam = lorentz<DIM>(P);
+    T w = g * P[1] + P[0];
+    U[0] = gam * P[0];
+    U[1] = (g - T(1)) * P[1] - sq(gam) * w;
+#pragma unroll
+    for (int m = 0; m < DIM; ++m) U[2 + m] = P[2 + m] * gam * w;
+}
+
+// function_PtoFx/Fy/Fz, src/3dim/structs.jl:99-142
+template <int DIM, typename T> VB_HD void prim2flux(int d, T g, const T* P, T* F) {
+    T gam = lorentz<DIM>(P);
+    T w = g * P[1] + P[0];
+    T un = P[2 + d];
+    F[0] = P[0] * un;
+    F[1] = -w * un * gam;
+#pragma unroll
+    for (int m = 0; m < DIM; ++m) {
+        if (m == d)
+            F[2 + m] = sq(un) * w + (g - T(1)) * P[1];
+        else
+            F[2 + m] = P[2 + m] * un * w;
+    }
+}
+
+// HARM signal speeds of one state, src/3dim/algos.jl:130-157
+template <int DIM, typename T> VB_HD void harm_speeds(int d, T g, const T* P, T& lp, T& lm) {
+    T lor = lorentz<DIM>(P);
+    T v = P[2 + d] / lor;
+    T C = sound_speed(P[0], P[1], g);
+    T sig = sq(C) / (sq(lor) * (T(1) - sq(C)));
+    T r = sqrt(sig * (T(1) - sq(v) + sig));
+    lp = (v + r) / (T(1) + sig);
+    lm = (v - r) / (T(1) + sig);
+}
+
+// HLL face flux, src/3dim/algos.jl:117-174 (states already floored)
+template <int DIM, typename T>
+VB_HD void hll_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
+    constexpr int NV = 2 + DIM;
+    T UL[NV], UR[NV], FL[NV], FR[NV];
+    prim2con<DIM>(g, PR, UR);
+    prim2con<DIM>(g, PL, UL);
+    prim2flux<DIM>(d, g, PR, FR);
+    prim2flux<DIM>(d, g, PL, FL);
+    T lpL, lmL, lpR, lmR;
+    harm_speeds<DIM>(d, g, PL, lpL, lmL);
+    harm_speeds<DIM>(d, g, PR, lpR, lmR);
+    T Cmax = jmax(lpL, lpR);
+    T Cmin = -jmin(lmL, lmR);
+    if (Cmax < T(0)) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Fo[v] = FR[v];
+    } else if (Cmin < T(0)) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Fo[v] = FL[v];
+    } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+            Fo[v] = (FR[v] * Cmin + FL[v] * Cmax - Cmax * Cmin * (UR[v] - UL[v])) / (Cmax + Cmin);
+    }
+}
+
+// HLLC face flux: an extension (the reference is HLL only). Mignone & Bodo
+// (2005, MNRAS 364, 126) relativistic HLLC with the HARM/Davis speed bounds
+// of the HLL above. Verona's conserved vector is (D, -E, m) and its flux
+// (D v_n, -m_n, m v_n + p e_n).
+template <int DIM, typename T>
+VB_HD void hllc_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
+    constexpr int NV = 2 + DIM;
+    T UL[NV], UR[NV], FL[NV], FR[NV];
+    prim2con<DIM>(g, PR, UR);
+    prim2con<DIM>(g, PL, UL);
+    prim2flux<DIM>(d, g, PR, FR);
+    prim2flux<DIM>(d, g, PL, FL);
+    T lpL, lmL, lpR, lmR;
+    harm_speeds<DIM>(d, g, PL, lpL, lmL);
+    harm_speeds<DIM>(d, g, PR, lpR, lmR);
+    T Cmax = jmax(lpL, lpR);
+    T Cmin = -jmin(lmL, lmR);
+    if (Cmax < T(0)) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Fo[v] = FR[v];
+        return;
+    }
+    if (Cmin < T(0)) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Fo[v] = FL[v];
+        return;
+    }
+    T lL = -Cmin, lR = Cmax;
+    T idl = T(1) / (lR - lL);
+    T E_L = -UL[1], E_R = -UR[1];
+    T m_L = UL[2 + d], m_R = UR[2 + d];
+    T FE_L = -FL[1], FE_R = -FR[1];
+    T Fm_L = FL[2 + d], Fm_R = FR[2 + d];
+    T E_h = (lR * E_R - lL * E_L - (FE_R - FE_L)) * idl;
+    T m_h = (lR * m_R - lL * m_L - (Fm_R - Fm_L)) * idl;
+    T FE_h = (lR * FE_L - lL * FE_R + lR * lL * (E_R - E_L)) * idl;
+    T Fm_h = (lR * Fm_L - lL * Fm_R + lR * lL * (m_R - m_L)) * idl;
+    T b = E_h + Fm_h;
+    T disc = b * b - T(4) * FE_h * m_h;
+    if (disc < T(0)) disc = T(0);
+    T ls = T(2) * m_h / (b + sqrt(disc));
+    T ps = Fm_h - FE_h * ls;
+    const bool left = ls >= T(0);
+    const T* P = left ? PL : PR;
+    const T* U = left ? UL : UR;
+    const T* F = left ? FL : FR;
+    T lK = left ? lL : lR;
+    T lor = lorentz<DIM>(P);
+    T vn = P[2 + d] / lor;
+    T p = (g - T(1)) * P[1];
+    T E = -U[1];
+    T fac = (lK - vn) / (lK - ls);
+    T Us[NV];
+    Us[0] = U[0] * fac;
+#pragma unroll
+    for (int m = 0; m < DIM; ++m) Us[2 + m] = U[2 + m] * fac;
+    Us[2 + d] = (U[2 + d] * (lK - vn) + ps - p) / (lK - ls);
+    T Es = (E * (lK - vn) + ps * ls - p * vn) / (lK - ls);
+    Us[1] = -Es;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Fo[v] = F[v] + lK * (Us[v] - U[v]);
+}
+
+template <int DIM, int RS, typename T>
+VB_HD void face_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
+    if (RS == RS_HLLC)
+        hllc_flux<DIM>(d, g, PL, PR, Fo);
+    else
+        hll_flux<DIM>(d, g, PL, PR, Fo);
+}
+
+// Largest |lambda| over the axes of one cell-centred state (CFL signal speed;
+// an extension -- the reference uses a fixed light-speed dt).
+template <int DIM, typename T> VB_HD T max_signal_speed(T g, const T* P) {
+    T c = T(0);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        T lp, lm;
+        harm_speeds<DIM>(d, g, P, lp, lm);
+        c = fmax(c, fmax(fabs(lp), fabs(lm)));
+    }
+    return c;
+}
+
+}  // namespace vb

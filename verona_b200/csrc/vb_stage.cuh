@@ -1,0 +1,549 @@
+// Fused RK-stage kernel and the small per-step kernels, templated on the
+// bulk type R of the primitive arrays (double: plain FP64; float: the FP32
+// bulk form, where U and con2prim stay FP64).
+//
+// Stage kernel (one launch per RK stage; replaces the reference's
+// Fluxes x/y/z + Update + UtoP + Limit launches, src/3dim/algos.jl:279-293):
+// a CTA owns a TX x TY x TZ tile of interior cells. For each axis it stages
+// the tile plus a 3-cell halo along that axis in shared memory, reconstructs
+// every cell ONCE (the reference evaluates WENOZ twice per face,
+// src/3dim/algos.jl:78,105), floors the face states, computes the face
+// fluxes in shared memory and accumulates the flux difference into per-cell
+// FP64 registers. Face states and fluxes never reach HBM. It then applies the
+// RK combination, solves con2prim with the cell's previous primitive state as
+// the guess and writes U and the floored P.
+#pragma once
+#include "vb_con2prim.cuh"
+#include "vb_internal.h"
+
+namespace vb {
+
+template <int DIM> struct TileCfg;
+template <> struct TileCfg<3> { static constexpr int TX = 32, TY = 4, TZ = 4, NT = 256; };
+template <> struct TileCfg<2> { static constexpr int TX = 32, TY = 8, TZ = 1, NT = 256; };
+template <> struct TileCfg<1> { static constexpr int TX = 256, TY = 1, TZ = 1, NT = 256; };
+
+template <int DIM, int TX, int TY, int TZ> struct TileGeom {
+    static constexpr int NV = 2 + DIM;
+    static constexpr int TC = TX * TY * TZ;
+    static constexpr int ext(int d) {
+        return (TX + (d == 0 ? 6 : 0)) * (TY + (d == 1 ? 6 : 0)) * (TZ + (d == 2 ? 6 : 0));
+    }
+    static constexpr int faces(int d) {
+        return (TX + (d == 0 ? 1 : 0)) * (TY + (d == 1 ? 1 : 0)) * (TZ + (d == 2 ? 1 : 0));
+    }
+    static constexpr int cmax(int a, int b) { return a > b ? a : b; }
+    static constexpr int EXTMAX = cmax(ext(0), cmax(DIM > 1 ? ext(1) : 0, DIM > 2 ? ext(2) : 0));
+    static constexpr int FACEMAX = cmax(faces(0), cmax(DIM > 1 ? faces(1) : 0, DIM > 2 ? faces(2) : 0));
+    template <typename R> static constexpr size_t smem_bytes() {
+        return sizeof(R) * NV * (size_t)(EXTMAX + 2 * FACEMAX);
+    }
+};
+
+__device__ __forceinline__ void count_add(unsigned long long* c, int which, unsigned long long v) {
+    if (c && v) atomicAdd(c + which, v);
+}
+
+// con2prim of one cell: per-dimension reference algorithm, or the W Newton
+// from a supplied guess with the bracketed fallback.
+template <int DIM>
+__device__ __forceinline__ int solve_cell(const StageParams& p, const double* U, double* P, long long gidx,
+                                          int& fallback) {
+    fallback = 0;
+    if (DIM == 3 && p.c2p_mode == C2P_GUESS_W) {
+        double W0;
+        if (p.w_guess) {
+            W0 = (double)p.w_guess[gidx];
+        } else {
+            double gm2 = sq(P[2]) + sq(P[3]) + sq(P[4]) + 1.0;
+            W0 = (P[0] + p.gamma * P[1]) * gm2;
+        }
+        int fb;
+        int it = c2p_w(p.gamma, U, W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, P, &fb);
+        fallback = fb;
+        return it;
+    }
+    if (DIM == 1) return c2p_1d(p.gamma, p.n_iter, p.tol, U, P);
+    if (DIM == 2) return c2p_2d(p.gamma, p.n_iter, p.tol, U, P);
+    int r = c2p_3d(p.gamma, p.n_iter, p.tol, U, P);
+    fallback = r > 1;
+    return r;
+}
+
+template <int DIM, int REC, int RS, typename R, int TX, int TY, int TZ, int NT>
+__global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
+    using G = TileGeom<DIM, TX, TY, TZ>;
+    constexpr int NV = G::NV;
+    constexpr int TC = G::TC;
+    constexpr int CPT = (TC + NT - 1) / NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* sP = reinterpret_cast<R*>(smem_raw);
+    R* sL = sP + NV * G::EXTMAX;
+    R* sR = sL + NV * G::FACEMAX;
+
+    const int tid = threadIdx.x;
+    const int T[3] = {TX, TY, TZ};
+    const int org[3] = {NG + (int)blockIdx.x * TX, DIM > 1 ? NG + (int)blockIdx.y * TY : 0,
+                        DIM > 2 ? NG + (int)blockIdx.z * TZ : 0};
+    // valid cells of this (possibly partial) tile along each axis
+    int vt[3];
+    for (int a = 0; a < 3; ++a) vt[a] = a < DIM ? min(T[a], p.n[a] - NG - org[a]) : 1;
+    const long long vs = p.vs;
+    const R fl = R(p.floor_);
+    const R g = R(p.gamma);
+
+    double acc[CPT][NV];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        int cell = tid + c * NT;
+        int lx = cell % TX, ly = (cell / TX) % TY, lz = cell / (TX * TY);
+        bool ok = cell < TC && lx < vt[0] && ly < vt[1] && lz < vt[2];
+        long long gidx = (org[0] + lx) + p.sy * (org[1] + ly) + p.sz * (org[2] + lz);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[c][v] = ok ? b.Us[v * vs + gidx] : 0.0;
+    }
+
+#pragma unroll 1
+    for (int d = 0; d < DIM; ++d) {
+        const int EX = TX + (d == 0 ? 6 : 0), EY = TY + (d == 1 ? 6 : 0), EZ = TZ + (d == 2 ? 6 : 0);
+        const int EXT = EX * EY * EZ;
+        const int ox = org[0] - (d == 0 ? NG : 0), oy = org[1] - (d == 1 ? NG : 0),
+                  oz = org[2] - (d == 2 ? NG : 0);
+        __syncthreads();
+        // 1. stage the axis-extended tile of P
+        for (int e = tid; e < NV * EXT; e += NT) {
+            int v = e / EXT, r = e - v * EXT;
+            int ex = r % EX, ey = (r / EX) % EY, ez = r / (EX * EY);
+            int gi = ox + ex, gj = oy + ey, gk = oz + ez;
+            R val = R(0);
+            if (gi < p.n[0] && gj < p.n[1] && gk < p.n[2]) val = b.Pin[v * vs + gi + p.sy * gj + p.sz * gk];
+            sP[v * EXT + r] = val;
+        }
+        __syncthreads();
+        // 2. reconstruct each cell of the tile (plus one halo cell on each side
+        //    along d) once; store its two face values, floored
+        const int FX = TX + (d == 0), FY = TY + (d == 1), FZ = TZ + (d == 2);
+        const int NF = FX * FY * FZ;
+        const int RX = TX + (d == 0 ? 2 : 0), RY = TY + (d == 1 ? 2 : 0), RZ = TZ + (d == 2 ? 2 : 0);
+        const int sd = d == 0 ? 1 : (d == 1 ? EX : EX * EY);
+        const int Td = T[d];
+        for (int e = tid; e < RX * RY * RZ; e += NT) {
+            int rx = e % RX, ry = (e / RX) % RY, rz = e / (RX * RY);
+            int c[3] = {rx - (d == 0), ry - (d == 1), rz - (d == 2)};
+            bool ok = true;
+            for (int a = 0; a < 3; ++a)
+                ok = ok && (a == d ? (c[a] >= -1 && c[a] <= vt[a]) : c[a] < vt[a]);
+            if (!ok) continue;
+            int ex = c[0] + (d == 0 ? NG : 0), ey = c[1] + (d == 1 ? NG : 0), ez = c[2] + (d == 2 ? NG : 0);
+            int base = ex + EX * (ey + EY * ez);
+            int fR = c[0] + FX * (c[1] + FY * c[2]);                    // face c_d
+            int fL = fR + (d == 0 ? 1 : (d == 1 ? FX : FX * FY));         // face c_d + 1
+            bool wR = c[d] >= 0, wL = c[d] + 1 <= vt[d];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const R* q = sP + v * EXT + base;
+                R qr, ql;
+                recon<REC>(q[-2 * sd], q[-sd], q[0], q[sd], q[2 * sd], qr, ql);
+                if (v < 2) {
+                    qr = jmax(fl, qr);
+                    ql = jmax(fl, ql);
+                }
+                if (wR) sR[v * NF + fR] = qr;
+                if (wL) sL[v * NF + fL] = ql;
+            }
+        }
+        __syncthreads();
+        // 3. face fluxes (overwrite the left states)
+        for (int e = tid; e < NF; e += NT) {
+            int f[3] = {e % FX, (e / FX) % FY, e / (FX * FY)};
+            bool ok = true;
+            for (int a = 0; a < 3; ++a) ok = ok && (a == d ? f[a] <= vt[a] : f[a] < vt[a]);
+            if (!ok) continue;
+            R PL[NV], PR[NV], F[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                PL[v] = sL[v * NF + e];
+                PR[v] = sR[v * NF + e];
+            }
+            face_flux<DIM, RS>(d, g, PL, PR, F);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) sL[v * NF + e] = F[v];
+        }
+        __syncthreads();
+        // 4. flux difference, in the reference's order x, y, z
+        const double cdt = p.dtdx[d];
+        const int fstep = d == 0 ? 1 : (d == 1 ? FX : FX * FY);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            int cell = tid + c * NT;
+            int lx = cell % TX, ly = (cell / TX) % TY, lz = cell / (TX * TY);
+            if (!(cell < TC && lx < vt[0] && ly < vt[1] && lz < vt[2])) continue;
+            int flo = lx + FX * (ly + FY * lz);
+#pragma unroll
+            for (int v = 0; v < NV; ++v)
+                acc[c][v] = acc[c][v] - cdt * ((double)sL[v * NF + flo + fstep] - (double)sL[v * NF + flo]);
+        }
+        (void)Td;
+    }
+
+    // 5. RK combination, con2prim (guess = this stage's input P), Limit
+    unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        int cell = tid + c * NT;
+        int lx = cell % TX, ly = (cell / TX) % TY, lz = cell / (TX * TY);
+        if (!(cell < TC && lx < vt[0] && ly < vt[1] && lz < vt[2])) continue;
+        long long gidx = (org[0] + lx) + p.sy * (org[1] + ly) + p.sz * (org[2] + lz);
+        double U[NV], P[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            double u = acc[c][v];
+            if (p.rk_a != 0.0) u = p.rk_a * b.U0[v * vs + gidx] + p.rk_b * u;
+            U[v] = u;
+            b.Uo[v * vs + gidx] = u;
+            P[v] = (double)b.Pin[v * vs + gidx];
+        }
+        int fb;
+        int r = solve_cell<DIM>(p, U, P, gidx, fb);
+        n_fail += (r < 0);
+        n_fb += fb;
+        n_it += (r < 0 ? -r : r);
+        n_cells += 1;
+        P[0] = jmax(P[0], p.floor_);
+        P[1] = jmax(P[1], p.floor_);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) b.Pout[v * vs + gidx] = (R)P[v];
+    }
+    if (n_fail) count_add(p.counters, CNT_C2P_FAIL, n_fail);
+    if (p.stats) {
+        // warp-aggregate the statistics; every thread of the CTA reaches here
+        for (int o = 16; o > 0; o >>= 1) {
+            n_fb += __shfl_xor_sync(0xffffffffu, n_fb, o);
+            n_it += __shfl_xor_sync(0xffffffffu, n_it, o);
+            n_cells += __shfl_xor_sync(0xffffffffu, n_cells, o);
+        }
+        if ((tid & 31) == 0) {
+            count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
+            count_add(p.counters, CNT_C2P_ITERS, n_it);
+            count_add(p.counters, CNT_C2P_CELLS, n_cells);
+        }
+    } else if (n_fb) {
+        count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
+    }
+}
+
+template <int DIM, int REC, int RS, typename R>
+cudaError_t launch_stage_t(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
+    using C = TileCfg<DIM>;
+    using G = TileGeom<DIM, C::TX, C::TY, C::TZ>;
+    auto kern = k_stage<DIM, REC, RS, R, C::TX, C::TY, C::TZ, C::NT>;
+    const size_t smem = G::template smem_bytes<R>();
+    static unsigned long long attr_set = 0;  // one bit per device, per instantiation
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(attr_set >> (dev & 63) & 1ULL)) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_set |= 1ULL << (dev & 63);
+    }
+    dim3 grid((p.n[0] - 2 * NG + C::TX - 1) / C::TX, DIM > 1 ? (p.n[1] - 2 * NG + C::TY - 1) / C::TY : 1,
+              DIM > 2 ? (p.n[2] - 2 * NG + C::TZ - 1) / C::TZ : 1);
+    kern<<<grid, C::NT, smem, s>>>(p, b);
+    return cudaGetLastError();
+}
+
+template <int DIM, typename R>
+cudaError_t dispatch_stage_dim(int rec, int rs, const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
+#define VB_CASE(RC, RSC)                                                                      \
+    if (rec == RC && rs == RSC) return launch_stage_t<DIM, RC, RSC, R>(p, b, s);
+    VB_CASE(REC_MINMOD, RS_HLL)
+    VB_CASE(REC_MINMOD, RS_HLLC)
+    VB_CASE(REC_PPM, RS_HLL)
+    VB_CASE(REC_PPM, RS_HLLC)
+    VB_CASE(REC_WENOZ, RS_HLL)
+    VB_CASE(REC_WENOZ, RS_HLLC)
+#undef VB_CASE
+    return cudaErrorInvalidValue;
+}
+
+template <typename R>
+cudaError_t launch_stage(int dims, int rec, int rs, const StageParams& p, const StageBufs<R>& b,
+                         cudaStream_t s) {
+    if (dims == 1) return dispatch_stage_dim<1, R>(rec, rs, p, b, s);
+    if (dims == 2) return dispatch_stage_dim<2, R>(rec, rs, p, b, s);
+    if (dims == 3) return dispatch_stage_dim<3, R>(rec, rs, p, b, s);
+    return cudaErrorInvalidValue;
+}
+
+// ---- layout conversion -----------------------------------------------------
+// One thread per cell; AoS reads of nv consecutive doubles, SoA writes are
+// coalesced per variable.
+template <int DIM, typename R>
+__global__ void k_load_prims(Grid g, const double* __restrict__ Pa, R* __restrict__ P, double* __restrict__ U0,
+                             double gamma) {
+    constexpr int NV = 2 + DIM;
+    long long ncell = (long long)g.n[0] * g.n[1] * g.n[2];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        double q[NV], u[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) q[v] = Pa[c * NV + v];
+        prim2con<DIM>(gamma, q, u);  // kernel_PtoU, src/3dim/structs.jl:66-81
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            P[v * g.vs + c] = (R)q[v];
+            U0[v * g.vs + c] = u[v];
+        }
+    }
+}
+
+template <int DIM, typename R>
+__global__ void k_store_prims(Grid g, const R* __restrict__ P, double* __restrict__ Pa) {
+    constexpr int NV = 2 + DIM;
+    long long ncell = (long long)g.n[0] * g.n[1] * g.n[2];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Pa[c * NV + v] = (double)P[v * g.vs + c];
+    }
+}
+
+inline int grid_for(long long n, int nt) {
+    long long b = (n + nt - 1) / nt;
+    if (b > 148LL * 32) b = 148LL * 32;
+    return (int)(b < 1 ? 1 : b);
+}
+
+template <typename R>
+cudaError_t launch_load_prims(const Grid& g, const double* Pa, R* P, double* U0, double gamma, cudaStream_t s) {
+    long long ncell = (long long)g.n[0] * g.n[1] * g.n[2];
+    int nb = grid_for(ncell, 256);
+    if (g.dims == 1) k_load_prims<1, R><<<nb, 256, 0, s>>>(g, Pa, P, U0, gamma);
+    else if (g.dims == 2) k_load_prims<2, R><<<nb, 256, 0, s>>>(g, Pa, P, U0, gamma);
+    else k_load_prims<3, R><<<nb, 256, 0, s>>>(g, Pa, P, U0, gamma);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_store_prims(const Grid& g, const R* P, double* Pa, cudaStream_t s) {
+    long long ncell = (long long)g.n[0] * g.n[1] * g.n[2];
+    int nb = grid_for(ncell, 256);
+    if (g.dims == 1) k_store_prims<1, R><<<nb, 256, 0, s>>>(g, P, Pa);
+    else if (g.dims == 2) k_store_prims<2, R><<<nb, 256, 0, s>>>(g, P, Pa);
+    else k_store_prims<3, R><<<nb, 256, 0, s>>>(g, P, Pa);
+    return cudaGetLastError();
+}
+
+// ---- ghost cells -------------------------------------------------------------
+// The ghost region is covered by disjoint slabs: x-lo/x-hi over all (j,k);
+// y-lo/y-hi over interior i and all k; z-lo/z-hi over interior (i,j).
+__device__ __forceinline__ bool ghost_slab_cell(const Grid& g, int slab, long long e, int& i, int& j, int& k) {
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int a = slab / 2, side = slab % 2;
+    int ext[3];
+    int lo[3];
+    if (a == 0) {
+        ext[0] = NG; ext[1] = n1; ext[2] = n2;
+        lo[0] = side ? n0 - NG : 0; lo[1] = 0; lo[2] = 0;
+    } else if (a == 1) {
+        ext[0] = n0 - 2 * NG; ext[1] = NG; ext[2] = n2;
+        lo[0] = NG; lo[1] = side ? n1 - NG : 0; lo[2] = 0;
+    } else {
+        ext[0] = n0 - 2 * NG; ext[1] = n1 - 2 * NG; ext[2] = NG;
+        lo[0] = NG; lo[1] = NG; lo[2] = side ? n2 - NG : 0;
+    }
+    long long tot = (long long)ext[0] * ext[1] * ext[2];
+    if (e >= tot) return false;
+    i = lo[0] + (int)(e % ext[0]);
+    j = lo[1] + (int)((e / ext[0]) % ext[1]);
+    k = lo[2] + (int)(e / ((long long)ext[0] * ext[1]));
+    return true;
+}
+
+template <typename R>
+__global__ void k_ghost_limit(Grid g, const R* __restrict__ Pin, R* __restrict__ Pout, double floor_) {
+    const int slab = blockIdx.y;
+    const R fl = R(floor_);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;; e += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        if (!ghost_slab_cell(g, slab, e, i, j, k)) break;
+        long long c = i + g.sy * j + g.sz * k;
+        for (int v = 0; v < g.nv; ++v) {
+            R x = Pin[v * g.vs + c];
+            if (v < 2) x = jmax(x, fl);  // function_Limit, src/3dim/algos.jl:5-12
+            Pout[v * g.vs + c] = x;
+        }
+    }
+}
+
+template <typename R>
+cudaError_t launch_ghost_limit(const Grid& g, const R* Pin, R* Pout, double floor_, cudaStream_t s) {
+    long long maxslab = (long long)NG * g.n[1] * g.n[2];
+    if (g.dims > 1) maxslab = max(maxslab, (long long)NG * g.n[0] * g.n[2]);
+    if (g.dims > 2) maxslab = max(maxslab, (long long)NG * g.n[0] * g.n[1]);
+    dim3 grid(grid_for(maxslab, 256), 2 * g.dims);
+    k_ghost_limit<R><<<grid, 256, 0, s>>>(g, Pin, Pout, floor_);
+    return cudaGetLastError();
+}
+
+// Boundary fill of one face, the on-device replacement of the reference's
+// host-side `fun_bound` broadcasts (examples/Jet3D/HARM_jet_breakout.jl:131-158):
+// OUTFLOW copies the first interior cell into the 3 ghost layers over the
+// full padded extent of the other axes; NOZZLE holds a fixed state inside a
+// radius (cells, from a centre in the face plane) and is OUTFLOW outside.
+// par: NOZZLE {radius, c1, c2, rho, u, u1, u2, u3}.
+struct BCPar {
+    double v[8];
+};
+
+template <typename R>
+__global__ void k_bc_face(Grid g, R* __restrict__ P, int face, int kind, BCPar par) {
+    const int a = face / 2, side = face % 2;
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    int ext[3] = {n0, n1, n2};
+    ext[a] = NG;
+    long long tot = (long long)ext[0] * ext[1] * ext[2];
+    int b1 = (a + 1) % 3, b2 = (a + 2) % 3;
+    if (b1 > b2) {
+        int t = b1;
+        b1 = b2;
+        b2 = t;
+    }
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        int idx[3] = {(int)(e % ext[0]), (int)((e / ext[0]) % ext[1]), (int)(e / ((long long)ext[0] * ext[1]))};
+        if (side) idx[a] += g.n[a] - NG;
+        long long c = idx[0] + g.sy * idx[1] + g.sz * idx[2];
+        bool inside = false;
+        if (kind == 2) {
+            double y1 = (b1 < g.dims) ? (idx[b1] - NG + 0.5) - par.v[1] : 0.0;
+            double y2 = (b2 < g.dims) ? (idx[b2] - NG + 0.5) - par.v[2] : 0.0;
+            inside = y1 * y1 + y2 * y2 < par.v[0] * par.v[0];
+        }
+        if (inside) {
+            P[c] = (R)par.v[3];
+            P[g.vs + c] = (R)par.v[4];
+            for (int m = 0; m < g.dims; ++m) P[(2 + m) * g.vs + c] = (R)par.v[5 + m];
+        } else {
+            int s[3] = {idx[0], idx[1], idx[2]};
+            s[a] = side ? g.n[a] - NG - 1 : NG;
+            long long cs = s[0] + g.sy * s[1] + g.sz * s[2];
+            for (int v = 0; v < g.nv; ++v) P[v * g.vs + c] = P[v * g.vs + cs];
+        }
+    }
+}
+
+template <typename R>
+cudaError_t launch_bc_face(const Grid& g, R* P, int face, int kind, const double* par, cudaStream_t s) {
+    BCPar bp;
+    for (int i = 0; i < 8; ++i) bp.v[i] = par ? par[i] : 0.0;
+    int a = face / 2;
+    long long tot = (long long)g.n[0] * g.n[1] * g.n[2] / g.n[a] * NG;
+    k_bc_face<R><<<grid_for(tot, 256), 256, 0, s>>>(g, P, face, kind, bp);
+    return cudaGetLastError();
+}
+
+// P[var, ghosts of face] *= factor (the engine decay of TurnOff,
+// examples/Jet3D/HARM_jet_breakout.jl:132-135)
+template <typename R>
+__global__ void k_bc_decay(Grid g, R* __restrict__ P, int face, int var, double factor) {
+    const int a = face / 2, side = face % 2;
+    int ext[3] = {g.n[0], g.n[1], g.n[2]};
+    ext[a] = NG;
+    long long tot = (long long)ext[0] * ext[1] * ext[2];
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        int idx[3] = {(int)(e % ext[0]), (int)((e / ext[0]) % ext[1]), (int)(e / ((long long)ext[0] * ext[1]))};
+        if (side) idx[a] += g.n[a] - NG;
+        long long c = idx[0] + g.sy * idx[1] + g.sz * idx[2];
+        P[var * g.vs + c] = (R)((double)P[var * g.vs + c] * factor);
+    }
+}
+
+template <typename R>
+cudaError_t launch_bc_decay(const Grid& g, R* P, int face, int var, double factor, cudaStream_t s) {
+    int a = face / 2;
+    long long tot = (long long)g.n[0] * g.n[1] * g.n[2] / g.n[a] * NG;
+    k_bc_decay<R><<<grid_for(tot, 256), 256, 0, s>>>(g, P, face, var, factor);
+    return cudaGetLastError();
+}
+
+// ---- CFL signal speed: per-thread max, warp-shuffle max, block max ----------
+constexpr int MS_THREADS = 256;
+
+__device__ __forceinline__ double warp_max(double x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    return x;
+}
+
+__device__ __forceinline__ double block_max(double x) {
+    __shared__ double red[MS_THREADS / 32];
+    x = warp_max(x);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        x = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        x = warp_max(x);
+    }
+    return x;
+}
+
+template <int DIM, typename R>
+__global__ void __launch_bounds__(MS_THREADS) k_max_speed(Grid g, const R* __restrict__ P, double gamma,
+                                                          double* __restrict__ partial) {
+    constexpr int NV = 2 + DIM;
+    const int N0 = g.n[0] - 2 * NG;
+    const int N1 = DIM > 1 ? g.n[1] - 2 * NG : 1;
+    const int N2 = DIM > 2 ? g.n[2] - 2 * NG : 1;
+    const long long tot = (long long)N0 * N1 * N2;
+    double m = 0.0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(e % N0) + NG;
+        int j = DIM > 1 ? (int)((e / N0) % N1) + NG : 0;
+        int k = DIM > 2 ? (int)(e / ((long long)N0 * N1)) + NG : 0;
+        long long c = i + g.sy * j + g.sz * k;
+        double q[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) q[v] = (double)P[v * g.vs + c];
+        m = fmax(m, max_signal_speed<DIM>(gamma, q));
+    }
+    m = block_max(m);
+    if (threadIdx.x == 0) partial[blockIdx.x] = m;
+}
+
+static __global__ void __launch_bounds__(MS_THREADS) k_max_reduce(const double* __restrict__ partial, int n,
+                                                           double* __restrict__ out) {
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, partial[i]);
+    m = block_max(m);
+    if (threadIdx.x == 0) *out = m;
+}
+
+template <typename R>
+cudaError_t launch_max_speed(const Grid& g, const R* P, double gamma, double* partial, int max_partial,
+                             double* out, cudaStream_t s) {
+    int nb = min(max_speed_blocks(g), max_partial);
+    if (nb < 1) return cudaErrorInvalidValue;
+    if (g.dims == 1) k_max_speed<1, R><<<nb, MS_THREADS, 0, s>>>(g, P, gamma, partial);
+    else if (g.dims == 2) k_max_speed<2, R><<<nb, MS_THREADS, 0, s>>>(g, P, gamma, partial);
+    else k_max_speed<3, R><<<nb, MS_THREADS, 0, s>>>(g, P, gamma, partial);
+    k_max_reduce<<<1, MS_THREADS, 0, s>>>(partial, nb, out);
+    return cudaGetLastError();
+}
+
+// explicit instantiation of every launcher for one bulk type
+#define VB_INSTANTIATE_LAUNCHERS(R)                                                                      \
+    template cudaError_t launch_stage<R>(int, int, int, const StageParams&, const StageBufs<R>&,       \
+                                         cudaStream_t);                                               \
+    template cudaError_t launch_load_prims<R>(const Grid&, const double*, R*, double*, double,        \
+                                              cudaStream_t);                                          \
+    template cudaError_t launch_store_prims<R>(const Grid&, const R*, double*, cudaStream_t);        \
+    template cudaError_t launch_ghost_limit<R>(const Grid&, const R*, R*, double, cudaStream_t);      \
+    template cudaError_t launch_bc_face<R>(const Grid&, R*, int, int, const double*, cudaStream_t);  \
+    template cudaError_t launch_bc_decay<R>(const Grid&, R*, int, int, double, cudaStream_t);        \
+    template cudaError_t launch_max_speed<R>(const Grid&, const R*, double, double*, int, double*,   \
+                                             cudaStream_t);
+
+}  // namespace vb

@@ -1,0 +1,8 @@
+// FP32-bulk instantiation: primitive arrays, reconstruction, Riemann fluxes
+// and flux differences in FP32; conserved variables, the RK accumulation and
+// con2prim in FP64. Built with FMA contraction enabled.
+#include "vb_stage.cuh"
+
+namespace vb {
+VB_INSTANTIATE_LAUNCHERS(float)
+}  // namespace vb
