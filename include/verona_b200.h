@@ -160,6 +160,23 @@ int vb_memory_bytes(vb_handle h, uint64_t* bytes);
 int vb_profile_enable(vb_handle h, int enable);
 int vb_profile_read(vb_handle h, double* stage_ms, int64_t* stage_launches, int64_t* all_launches);
 
+/* ---- point kernels: the FP64 device physics on n independent states ----------
+ * Device pointers, struct-of-arrays: component k of point i at [k * n + i].
+ * They mirror the reference's scalar functions one to one and serve as the
+ * finest-grained parity seam. */
+/* reconstruction(::Val{M}, q_im2..q_ip2) -> (qr_i, ql_ip1), src/fluxlimiter.jl:183-200;
+ * q: 5 x n, out: 2 x n */
+int vb_point_recon(int method, const double* q, double* out, int n, void* stream);
+/* face flux of floored left/right primitive states along `axis` (HLL:
+ * src/3dim/algos.jl:117-174; HLLC: extension); PL, PR, F: (2+dims) x n */
+int vb_point_flux(int dims, int axis, int riemann, double gamma, const double* PL, const double* PR, double* F,
+                  int n, void* stream);
+/* con2prim per dimension (1D src/1dim/structs.jl:78-105, 2D src/2dim/structs.jl:249-330,
+ * 3D src/3dim/structs.jl:218-628); P holds the guess on entry; ret (may be NULL)
+ * receives the iteration count (1D/2D) or converged stage (3D), negative on failure */
+int vb_point_con2prim(int dims, double gamma, int n_iter, double tol, const double* U, double* P, int* ret, int n,
+                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -74,6 +74,9 @@ _SIGS = {
     "vb_memory_bytes": [_vp, C.POINTER(C.c_uint64)],
     "vb_profile_enable": [_vp, C.c_int],
     "vb_profile_read": [_vp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
+    "vb_point_recon": [C.c_int, _vp, _vp, C.c_int, _vp],
+    "vb_point_flux": [C.c_int, C.c_int, C.c_int, C.c_double, _vp, _vp, _vp, C.c_int, _vp],
+    "vb_point_con2prim": [C.c_int, C.c_double, C.c_int, C.c_double, _vp, _vp, _vp, C.c_int, _vp],
 }
 
 

@@ -529,4 +529,26 @@ int vb_memory_bytes(vb_handle h, uint64_t* bytes) {
     return VB_OK;
 }
 
+int vb_point_recon(int method, const double* q, double* out, int n, void* stream) {
+    if (!q || !out || n < 0 || method < 0 || method > 2) return fail(nullptr, VB_ERR_ARG, "vb_point_recon: bad argument");
+    VB_CUDA(nullptr, launch_point_recon(method, q, out, n, (cudaStream_t)stream));
+    return VB_OK;
+}
+
+int vb_point_flux(int dims, int axis, int riemann, double gamma, const double* PL, const double* PR, double* F, int n,
+                  void* stream) {
+    if (dims < 1 || dims > 3 || axis < 0 || axis >= dims || riemann < 0 || riemann > 1 || !PL || !PR || !F || n < 0)
+        return fail(nullptr, VB_ERR_ARG, "vb_point_flux: bad argument");
+    VB_CUDA(nullptr, launch_point_flux(dims, axis, riemann, gamma, PL, PR, F, n, (cudaStream_t)stream));
+    return VB_OK;
+}
+
+int vb_point_con2prim(int dims, double gamma, int n_iter, double tol, const double* U, double* P, int* ret, int n,
+                      void* stream) {
+    if (dims < 1 || dims > 3 || n_iter < 1 || !U || !P || n < 0)
+        return fail(nullptr, VB_ERR_ARG, "vb_point_con2prim: bad argument");
+    VB_CUDA(nullptr, launch_point_con2prim(dims, gamma, n_iter, tol, U, P, ret, n, (cudaStream_t)stream));
+    return VB_OK;
+}
+
 }  // extern "C"

@@ -87,4 +87,11 @@ cudaError_t launch_ref1d_store(const Ref1DState& st, double* P_aos, cudaStream_t
 
 int max_speed_blocks(const Grid& g);
 
+// point kernels (FP64, vb_stage_f64.cu)
+cudaError_t launch_point_recon(int method, const double* q, double* out, int n, cudaStream_t s);
+cudaError_t launch_point_flux(int dims, int axis, int rs, double g, const double* PL, const double* PR, double* F,
+                              int n, cudaStream_t s);
+cudaError_t launch_point_con2prim(int dims, double g, int n_iter, double tol, const double* U, double* P, int* ret,
+                                  int n, cudaStream_t s);
+
 }  // namespace vb

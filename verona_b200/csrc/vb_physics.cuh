@@ -301,14 +301,21 @@ VB_HD void hllc_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
     if (disc < T(0)) disc = T(0);
     T ls = T(2) * m_h / (b + sqrt(disc));
     T ps = Fm_h - FE_h * ls;
+    // star state of the side the contact leaves behind x/t = 0; values are
+    // selected one by one (no pointer to either side's arrays) so that every
+    // array stays in registers
     const bool left = ls >= T(0);
-    const T* P = left ? PL : PR;
-    const T* U = left ? UL : UR;
-    const T* F = left ? FL : FR;
+    T Pk[NV], U[NV], F[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        Pk[v] = left ? PL[v] : PR[v];
+        U[v] = left ? UL[v] : UR[v];
+        F[v] = left ? FL[v] : FR[v];
+    }
     T lK = left ? lL : lR;
-    T lor = lorentz<DIM>(P);
-    T vn = P[2 + d] / lor;
-    T p = (g - T(1)) * P[1];
+    T lor = lorentz<DIM>(Pk);
+    T vn = Pk[2 + d] / lor;
+    T p = (g - T(1)) * Pk[1];
     T E = -U[1];
     T fac = (lK - vn) / (lK - ls);
     T Us[NV];
