@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--n", type=int, default=512, help="interior cells per axis")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--path", default="both", choices=["both", "fast", "fp64"],
+                    help="fp64: time only the plain FP64 path (profiling runs)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
 
@@ -107,12 +109,18 @@ class Clocks:
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
-        self.index = index
+        self.index = str(index)
+        try:
+            import torch
+
+            self.index = "GPU-" + str(torch.cuda.get_device_properties(index).uuid)
+        except Exception:
+            pass
         self.p = None
 
     def __enter__(self):
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+            self.p = subprocess.Popen(["nvidia-smi", "-i", self.index, f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
@@ -218,7 +226,7 @@ def cpu_baseline(seconds):
     P[1] = 1e-3 / (GAMMA - 1)
     s = O.SolverND(3, n, P, GAMMA, 1e-8, 50, 1e-12, O.WENOZ, O.HLLC, 3)
     s.set_grid(1.0 / S, 1.0 / S, 1.0 / S)
-    s.set_boundary(0, O.BC_NOZZLE, [16.0 * S / 512 * 4, S / 2, S / 2, 0.01, 3e-3, 99 ** 0.5, 0, 0])
+    s.set_boundary(0, O.BC_NOZZLE, [16.0 * S / 512, S / 2, S / 2, 0.01, 3e-3, 99 ** 0.5, 0, 0])
     dt = dt_of(S)
     t0 = time.perf_counter()
     s.step(dt, 1)
@@ -276,7 +284,15 @@ def run_ours(args, rank, world, dist):
 
     # plain FP64 path (same scheme, reference con2prim)
     fp64 = None
-    if not args.no_fp64:
+    if args.path == "fp64":
+        s = make_solver(n, "fp64", "previous")
+        s.load_prims(P0)
+        ms, st_ms, st_l, ln = timed_steps(s, dt, W, K, dist)
+        print(json.dumps({"path": "fp64", "zone_updates_per_s": cells * K / (ms / 1e3), "ms_per_step": ms / K,
+                          "stage_ms_per_launch": st_ms / max(st_l, 1), "launches": ln}), flush=True)
+        s.close()
+        return
+    if not args.no_fp64 and args.path == "both":
         s = make_solver(n, "fp64", "previous")
         s.load_prims(P0)
         ms, st_ms, st_l, ln = timed_steps(s, dt, W, K, dist)
