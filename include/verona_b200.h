@@ -177,6 +177,25 @@ int vb_point_flux(int dims, int axis, int riemann, double gamma, const double* P
 int vb_point_con2prim(int dims, double gamma, int n_iter, double tol, const double* U, double* P, int* ret, int n,
                       void* stream);
 
+/* ---- allocation-free CFL reduction ----------------------------------------------
+ * No counterpart in the reference. The same maximum signal speed as
+ * vb_max_signal_speed, computed from a caller-owned device array in the
+ * reference layout (FP64 AoS, 3 ghosts per side) of an nx x ny x nz interior
+ * grid, written to the caller-owned device double *c_dev. For callers that
+ * cannot have the library allocate device memory (a host whose memory pool
+ * already owns the GPU, or code that must not trigger the implicit device
+ * synchronisation of cudaMalloc/cudaFree): it calls no allocator; its only
+ * scratch is a fixed 64 KiB array inside the library (8192 partial maxima),
+ * held on every GPU that loads the library until the process exits. The
+ * interior may have at most 8192 x 256 x 128 = 268,435,456 cells; larger
+ * grids are rejected with VB_ERR_ARG. The first call on a device looks up the
+ * scratch address on that device (make it before any stream capture). Calls
+ * share the scratch, so two calls whose kernels overlap on the GPU race.
+ * Errors: vb_noalloc_last_error(). */
+int vb_max_signal_speed_noalloc(int dims, int nx, int ny, int nz, double gamma, const double* P_aos_dev,
+                                double* c_dev, void* stream);
+const char* vb_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
