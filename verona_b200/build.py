@@ -3,7 +3,9 @@
 Translation units and their floating-point contract:
   vb_stage_f64.cu, vb_ref1d.cu, vb_api.cu  -fmad=false  (FP64 path rounds as
                                             the reference: no FMA contraction)
-  vb_stage_f32.cu                           -fmad=true   (FP32-bulk path)
+  vb_stage_f32.cu                           -fmad=true, approximate FP32 divide and
+                                            square root, FTZ (FP32-bulk path; the
+                                            FP64 con2prim in it stays IEEE)
   vb_mlp.cu                                 -fmad=true   (BF16 tensor-core MLP)
 Objects go to verona_b200/_build/, the library to verona_b200/libverona_b200.so.
 """
@@ -28,7 +30,7 @@ UNITS = {
     "vb_stage_f64.cu": ["-fmad=false"],
     "vb_ref1d.cu": ["-fmad=false"],
     "vb_api.cu": ["-fmad=false"],
-    "vb_stage_f32.cu": ["-fmad=true"],
+    "vb_stage_f32.cu": ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
 }
 
 

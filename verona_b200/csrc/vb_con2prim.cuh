@@ -193,12 +193,22 @@ VB_HD void prims_from_W(double g, double D, double Qx, double Qy, double Qz, dou
     P[4] = gm * Qz / W;
 }
 
+#ifdef __CUDA_ARCH__
+#define VB_NOINLINE __noinline__
+#else
+#define VB_NOINLINE
+#endif
+
+static VB_NOINLINE __host__ __device__ int c2p_3d_tail(double g, int n_iter, double tol, const double* Uc, double* P);
+
 // 3D function_UtoP, src/3dim/structs.jl:258-620: 1DW Newton -> Noble 2D
 // Newton with line search -> 5x5 primitive Newton -> bisection. Returns the
 // stage that converged (1..4) or -1 (cell set to NaN, as the reference does).
+// The 1DW stage, which converges for almost every cell, is inline; the rest
+// of the cascade (c2p_3d_tail) is an out-of-line call so that its registers
+// do not count against the stencil kernels.
 VB_HD int c2p_3d(double g, int n_iter, double tol, const double* Uc, double* P) {
     const double D = Uc[0], Q_t = Uc[1], Q_x = Uc[2], Q_y = Uc[3], Q_z = Uc[4];
-    bool conv1 = false, conv2 = false, conv5 = false, convb = false;
     double S2, W, v2;
     {
         S2 = Q_x * Q_x + Q_y * Q_y + Q_z * Q_z;
@@ -229,12 +239,22 @@ VB_HD int c2p_3d(double g, int n_iter, double tol, const double* Uc, double* P) 
                 W = Wp;
             if (dW < 0) dW = -dW;
             if (sq(dW) < sq(tol)) {
-                conv1 = true;
-                break;
+                prims_from_W(g, D, Q_x, Q_y, Q_z, S2, W, P);
+                return 1;
             }
         }
     }
-    if (!conv1) {
+    return c2p_3d_tail(g, n_iter, tol, Uc, P);
+}
+
+// Stages 2-4 of the 3D cascade (src/3dim/structs.jl:345-619), entered when
+// the 1DW Newton did not converge; P still holds the guess.
+static VB_NOINLINE __host__ __device__ int c2p_3d_tail(double g, int n_iter, double tol, const double* Uc, double* P) {
+    const double D = Uc[0], Q_t = Uc[1], Q_x = Uc[2], Q_y = Uc[3], Q_z = Uc[4];
+    const bool conv1 = false;
+    bool conv2 = false, conv5 = false, convb = false;
+    double S2, W, v2;
+    {
         S2 = Q_x * Q_x + Q_y * Q_y + Q_z * Q_z;
         double gm = sqrt(sq(P[2]) + sq(P[3]) + sq(P[4]) + 1.0);
         double w_small = P[0] + g * P[1];

@@ -35,6 +35,7 @@ struct StageParams {
     int w_max_newton;    // C2P_GUESS_W: Newton steps before the bracketed fallback
     const float* w_guess;  // C2P_GUESS_W: per-cell W guesses (nullptr: derive from Pin)
     unsigned long long* counters;
+    int force_box;       // 1: use the box-tile kernel even where the z-marching one fits
 };
 
 template <typename R> struct StageBufs {

@@ -266,12 +266,21 @@ cudaError_t dispatch_stage_dim(int rec, int rs, const StageParams& p, const Stag
     return cudaErrorInvalidValue;
 }
 
+template <typename R> inline bool zm_fits(const StageParams& p);
+template <typename R>
+cudaError_t dispatch_stage_zm(int rec, int rs, const StageParams& p, const StageBufs<R>& b, cudaStream_t s);
+
+// 3D grids whose x/y interior extents are multiples of the z-marching tile
+// use k_stage_zm; everything else (1D, 2D, ragged 3D) the box-tile k_stage.
 template <typename R>
 cudaError_t launch_stage(int dims, int rec, int rs, const StageParams& p, const StageBufs<R>& b,
                          cudaStream_t s) {
     if (dims == 1) return dispatch_stage_dim<1, R>(rec, rs, p, b, s);
     if (dims == 2) return dispatch_stage_dim<2, R>(rec, rs, p, b, s);
-    if (dims == 3) return dispatch_stage_dim<3, R>(rec, rs, p, b, s);
+    if (dims == 3) {
+        if (zm_fits<R>(p) && !p.force_box) return dispatch_stage_zm<R>(rec, rs, p, b, s);
+        return dispatch_stage_dim<3, R>(rec, rs, p, b, s);
+    }
     return cudaErrorInvalidValue;
 }
 

@@ -2,6 +2,7 @@
 // and flux differences in FP32; conserved variables, the RK accumulation and
 // con2prim in FP64. Built with FMA contraction enabled.
 #include "vb_stage.cuh"
+#include "vb_stage_zm.cuh"
 
 namespace vb {
 VB_INSTANTIATE_LAUNCHERS(float)

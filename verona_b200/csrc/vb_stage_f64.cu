@@ -1,6 +1,7 @@
 // Plain FP64 instantiation of the stage and per-step kernels. Built with
 // -fmad=false so every operation rounds as the reference's Julia code does.
 #include "vb_stage.cuh"
+#include "vb_stage_zm.cuh"
 
 namespace vb {
 VB_INSTANTIATE_LAUNCHERS(double)
