@@ -148,6 +148,19 @@ int vb_max_signal_speed(vb_handle h, double* c, void* stream);
 int vb_get_counters(vb_handle h, uint64_t* out, int n, void* stream);
 int vb_reset_counters(vb_handle h, void* stream);
 
+/* Kernel variants (no counterpart in the reference; see verona_b200/autotune.py).
+ * split_con2prim: 1 = the 3D stencil kernel writes U and a separate
+ * barrier-free kernel solves con2prim; 0 = one fused kernel; -1 = library
+ * default. force_box: 1 = use the box-tile stencil kernel for 3D even where
+ * the z-marching kernel fits. Results are identical for every variant. */
+typedef struct vb_tuning {
+    int32_t split_con2prim;
+    int32_t force_box;
+    int32_t reserved[6];
+} vb_tuning;
+int vb_set_tuning(vb_handle h, const vb_tuning* t);
+int vb_get_tuning(vb_handle h, vb_tuning* t);
+
 /* Device bytes held by the handle. */
 int vb_memory_bytes(vb_handle h, uint64_t* bytes);
 

@@ -256,7 +256,8 @@ def test_errors_are_reported_not_trapped():
 @pytest.mark.parametrize("rec", [0, 1, 2])
 @pytest.mark.parametrize("rs", [0, 1])
 @pytest.mark.parametrize("rk", [2, 3])
-def test_zmarch_kernel_parity(oracle, rec, rs, rk):
+@pytest.mark.parametrize("variant", ["fused", "split", "box"])
+def test_zmarch_kernel_parity(oracle, rec, rs, rk, variant):
     """3D grids with x/y extents that are multiples of the 32x8 tile run the
     z-marching kernel; 70 cells in z make two z-ranges, the second partial."""
     from verona_b200 import Solver
@@ -268,6 +269,7 @@ def test_zmarch_kernel_parity(oracle, rec, rs, rk):
     dt = 0.4 / sum(1.0 / d for d in dxs)
     noz = nozzle_params(3, n, 5.0, gamma=g)
     s = Solver(3, n, g, dxs, recon=rec, riemann=rs, rk=rk, n_iter=50, tol=1e-12, floor=1e-8)
+    s.set_tuning(split_con2prim=int(variant == "split"), force_box=int(variant == "box"))
     s.set_boundary(0, 2, noz)
     s.load_prims(P0)
     s.step(dt, 2)

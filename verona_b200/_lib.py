@@ -42,6 +42,10 @@ class VBOptions(C.Structure):
     ]
 
 
+class VBTuning(C.Structure):
+    _fields_ = [("split_con2prim", C.c_int32), ("force_box", C.c_int32), ("reserved", C.c_int32 * 6)]
+
+
 class VBError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"verona_b200 error {code}: {msg}")
@@ -74,6 +78,8 @@ _SIGS = {
     "vb_memory_bytes": [_vp, C.POINTER(C.c_uint64)],
     "vb_profile_enable": [_vp, C.c_int],
     "vb_profile_read": [_vp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
+    "vb_set_tuning": [_vp, C.POINTER(VBTuning)],
+    "vb_get_tuning": [_vp, C.POINTER(VBTuning)],
     "vb_point_recon": [C.c_int, _vp, _vp, C.c_int, _vp],
     "vb_point_flux": [C.c_int, C.c_int, C.c_int, C.c_double, _vp, _vp, _vp, C.c_int, _vp],
     "vb_point_con2prim": [C.c_int, C.c_double, C.c_int, C.c_double, _vp, _vp, _vp, C.c_int, _vp],

@@ -50,6 +50,8 @@ struct vb_solver {
     double* staging = nullptr;
     size_t bytes = 0;
     std::string err;
+    // kernel variants
+    vb_tuning tun{-1, 0, {0, 0, 0, 0, 0, 0}};
     // profiling
     bool prof = false;
     std::vector<cudaEvent_t> ev;
@@ -377,6 +379,9 @@ template <typename R> static int bc_fill(vb_handle h, R* P, cudaStream_t s) {
     return VB_OK;
 }
 
+// split con2prim by default where it measured faster (3D)
+static int default_split(const vb_solver* h) { return h->dims == 3 ? 1 : 0; }
+
 template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s) {
     Grid g = grid_of(h);
     R* P[2] = {(R*)h->P[0], (R*)h->P[1]};
@@ -398,6 +403,8 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
     p.w_max_newton = h->opt.w_max_newton;
     p.w_guess = nullptr;
     p.counters = h->cnt;
+    p.force_box = h->tun.force_box;
+    p.split = h->tun.split_con2prim < 0 ? default_split(h) : h->tun.split_con2prim;
     auto stage = [&](const R* Pin, R* Pout, const double* Us, double* Uo, double dts, double a, double b) -> int {
         for (int d = 0; d < 3; ++d) p.dtdx[d] = d < h->dims ? dts / h->dx[d] : 0.0;
         p.rk_a = a;
@@ -412,7 +419,7 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
         VB_CUDA(h, launch_stage<R>(h->dims, h->opt.recon, h->opt.riemann, p, bufs, s));
         if (h->prof) VB_CUDA(h, cudaEventRecord(e1, s));
         VB_CUDA(h, launch_ghost_limit<R>(g, Pin, Pout, h->opt.floor_, s));
-        h->launches += 2;
+        h->launches += 2 + (p.split && h->dims == 3 ? 1 : 0);
         h->stage_launches += 1;
         return VB_OK;
     };
@@ -520,6 +527,20 @@ int vb_profile_read(vb_handle h, double* stage_ms, int64_t* stage_launches, int6
     *all_launches = h->launches;
     h->ev_used = 0;
     h->launches = h->stage_launches = 0;
+    return VB_OK;
+}
+
+int vb_set_tuning(vb_handle h, const vb_tuning* t) {
+    if (!h || !t) return fail(h, VB_ERR_ARG, "vb_set_tuning: null argument");
+    if (t->split_con2prim < -1 || t->split_con2prim > 1 || t->force_box < 0 || t->force_box > 1)
+        return fail(h, VB_ERR_ARG, "vb_set_tuning: split_con2prim in {-1,0,1}, force_box in {0,1}");
+    h->tun = *t;
+    return VB_OK;
+}
+
+int vb_get_tuning(vb_handle h, vb_tuning* t) {
+    if (!h || !t) return fail(h, VB_ERR_ARG, "vb_get_tuning: null argument");
+    *t = h->tun;
     return VB_OK;
 }
 

@@ -36,6 +36,7 @@ struct StageParams {
     const float* w_guess;  // C2P_GUESS_W: per-cell W guesses (nullptr: derive from Pin)
     unsigned long long* counters;
     int force_box;       // 1: use the box-tile kernel even where the z-marching one fits
+    int split;           // 1: z-marching stencil kernel writes U only; k_c2p solves con2prim
 };
 
 template <typename R> struct StageBufs {

@@ -70,7 +70,7 @@ __device__ __forceinline__ void recon_floored(const R* q, int s, R fl, int v, R&
     }
 }
 
-template <int REC, int RS, typename R, int TX, int TY, int LZ, int MINB>
+template <int REC, int RS, typename R, int TX, int TY, int LZ, int MINB, bool SPLIT>
 __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zm(StageParams p, StageBufs<R> b) {
     using G = ZmGeom<TX, TY>;
     constexpr int NV = 5, NT = G::NT, EX = G::EX, PLN = G::PLN, FN = G::FN, QXN = G::QXN;
@@ -272,8 +272,16 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zm(StageParams p, Stage
 #pragma unroll
         for (int v = 0; v < NV; ++v) nxt[v] = has_next ? b.Pin[v * vs + c + 4 * sz] : R(0);
 
-        // RK combination, con2prim (guess = plane k of this stage's P), Limit
-        {
+        // RK combination, con2prim (guess = plane k of this stage's P), Limit;
+        // in split mode only U is written here and k_c2p finishes the cell
+        if (SPLIT) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                double u = acc.result(v, b.Us, vs, c);
+                if (p.rk_a != 0.0) u = p.rk_a * b.U0[v * vs + c] + p.rk_b * u;
+                b.Uo[v * vs + c] = u;
+            }
+        } else {
             double U[NV], P[NV];
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
@@ -317,19 +325,67 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zm(StageParams p, Stage
 
 // Tile shape of the z-marching kernel per bulk type.
 template <typename R> struct ZmCfg;
-template <> struct ZmCfg<float> { static constexpr int TX = 32, TY = 8, LZ = 64, MINB = 3; };
-template <> struct ZmCfg<double> { static constexpr int TX = 32, TY = 8, LZ = 64, MINB = 2; };
+template <> struct ZmCfg<float> { static constexpr int TX = 32, TY = 8, LZ = 64, MINB = 3, MINB_SPLIT = 4; };
+template <> struct ZmCfg<double> { static constexpr int TX = 32, TY = 8, LZ = 64, MINB = 2, MINB_SPLIT = 2; };
 
 template <typename R> inline bool zm_fits(const StageParams& p) {
     using C = ZmCfg<R>;
     return (p.n[0] - 2 * NG) % C::TX == 0 && (p.n[1] - 2 * NG) % C::TY == 0 && p.n[2] - 2 * NG >= 1;
 }
 
-template <int REC, int RS, typename R>
-cudaError_t launch_stage_zm(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
+// Split-mode con2prim: one thread per interior cell, no barriers, no shared
+// memory; reads the stage's U and the guess P, writes the floored P.
+template <typename R>
+__global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
+    constexpr int NV = 5;
+    const int N0 = p.n[0] - 2 * NG, N1 = p.n[1] - 2 * NG, N2 = p.n[2] - 2 * NG;
+    const long long tot = (long long)N0 * N1 * N2;
+    unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % N0) + NG;
+        const int j = (int)((e / N0) % N1) + NG;
+        const int k = (int)(e / ((long long)N0 * N1)) + NG;
+        const long long c = i + p.sy * j + p.sz * k;
+        double U[NV], P[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            U[v] = b.Uo[v * p.vs + c];
+            P[v] = (double)b.Pin[v * p.vs + c];
+        }
+        int fb;
+        int r = solve_cell<3>(p, U, P, c, fb);
+        n_fail += (r < 0);
+        n_fb += fb;
+        n_it += (r < 0 ? -r : r);
+        n_cells += 1;
+        P[0] = jmax(P[0], p.floor_);
+        P[1] = jmax(P[1], p.floor_);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) b.Pout[v * p.vs + c] = (R)P[v];
+    }
+    if (n_fail) count_add(p.counters, CNT_C2P_FAIL, n_fail);
+    if (p.stats) {
+        for (int o = 16; o > 0; o >>= 1) {
+            n_fb += __shfl_xor_sync(0xffffffffu, n_fb, o);
+            n_it += __shfl_xor_sync(0xffffffffu, n_it, o);
+            n_cells += __shfl_xor_sync(0xffffffffu, n_cells, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
+            count_add(p.counters, CNT_C2P_ITERS, n_it);
+            count_add(p.counters, CNT_C2P_CELLS, n_cells);
+        }
+    } else if (n_fb) {
+        count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
+    }
+}
+
+template <int REC, int RS, typename R, bool SPLIT>
+cudaError_t launch_stage_zm_t(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
     using C = ZmCfg<R>;
     using G = ZmGeom<C::TX, C::TY>;
-    auto kern = k_stage_zm<REC, RS, R, C::TX, C::TY, C::LZ, C::MINB>;
+    auto kern = k_stage_zm<REC, RS, R, C::TX, C::TY, C::LZ, SPLIT ? C::MINB_SPLIT : C::MINB, SPLIT>;
     const size_t smem = G::template smem_bytes<R>();
     static unsigned long long attr_set = 0;
     int dev = 0;
@@ -341,7 +397,16 @@ cudaError_t launch_stage_zm(const StageParams& p, const StageBufs<R>& b, cudaStr
     }
     dim3 grid((p.n[0] - 2 * NG) / C::TX, (p.n[1] - 2 * NG) / C::TY, (p.n[2] - 2 * NG + C::LZ - 1) / C::LZ);
     kern<<<grid, C::TX * C::TY, smem, s>>>(p, b);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !SPLIT) return e;
+    const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
+    k_c2p<R><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
     return cudaGetLastError();
+}
+
+template <int REC, int RS, typename R>
+cudaError_t launch_stage_zm(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
+    return p.split ? launch_stage_zm_t<REC, RS, R, true>(p, b, s) : launch_stage_zm_t<REC, RS, R, false>(p, b, s);
 }
 
 template <typename R>
