@@ -190,6 +190,40 @@ int vb_point_flux(int dims, int axis, int riemann, double gamma, const double* P
 int vb_point_con2prim(int dims, double gamma, int n_iter, double tol, const double* U, double* P, int* ret, int n,
                       void* stream);
 
+/* ---- learned con2prim guess (extension; the reference warm-starts Newton from
+ * the previous primitive state, src/3dim/structs.jl:277-287) ----------------------
+ * A 4 -> 64 -> 64 -> 64 -> 1 SiLU MLP in BF16 on the tensor cores (tcgen05, FP32
+ * accumulation in TMEM). Features f = (log D, log1p(|S|/D), log max(tau/D, 1e-12),
+ * Gamma) normalised by norm = {mean[4], 1/std[4]}; output y = log(p/D). Parameters
+ * are one FP32 vector of vb_mlp_param_count() values:
+ * W1[4][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] w4[64] b4 (W[in][out]).
+ * All array arguments are device pointers. */
+typedef struct vb_mlp* vb_mlp_handle;
+int vb_mlp_create(vb_mlp_handle* m);
+int vb_mlp_destroy(vb_mlp_handle m);
+const char* vb_mlp_last_error(vb_mlp_handle m);
+int vb_mlp_param_count(void);
+/* host arrays: params[vb_mlp_param_count()], norm[8] */
+int vb_mlp_set_params(vb_mlp_handle m, const float* params, const float* norm, void* stream);
+int vb_mlp_get_params(vb_mlp_handle m, float* params, float* norm, void* stream);
+/* features (n x 4) and, if P != NULL, targets log(p/D) (n) of n conserved states U
+ * (5 x n, FP64 struct-of-arrays; P likewise) */
+int vb_mlp_features(vb_mlp_handle m, const double* U, const double* P, int n, double gamma, float* feat,
+                    float* target, void* stream);
+/* tensor-core inference: out[n] = y(feat) */
+int vb_mlp_forward(vb_mlp_handle m, const float* feat, int n, float* out, void* stream);
+/* one optimisation step on n samples (mean squared error on y): forward and
+ * backward on the tensor cores, then Adam with learning rate lr (lr = 0:
+ * gradients only); *loss (may be NULL) receives the batch loss. Synchronises
+ * when loss != NULL. */
+int vb_mlp_train_step(vb_mlp_handle m, const float* feat, const float* target, int n, float lr, float* loss,
+                      void* stream);
+/* host copy of the gradient of the last step (same layout as the parameters) */
+int vb_mlp_get_grad(vb_mlp_handle m, float* grad, void* stream);
+/* use the network as the con2prim guess of a 3D solver (options.guess =
+ * VB_GUESS_LEARNED); the network must outlive the solver's use of it */
+int vb_attach_mlp(vb_handle h, vb_mlp_handle m);
+
 /* ---- allocation-free CFL reduction ----------------------------------------------
  * No counterpart in the reference. The same maximum signal speed as
  * vb_max_signal_speed, computed from a caller-owned device array in the
@@ -208,6 +242,14 @@ int vb_point_con2prim(int dims, double gamma, int n_iter, double tol, const doub
 int vb_max_signal_speed_noalloc(int dims, int nx, int ny, int nz, double gamma, const double* P_aos_dev,
                                 double* c_dev, void* stream);
 const char* vb_noalloc_last_error(void);
+
+/* The learned path's refinement on n 3D states: Newton on W from the guesses
+ * W0 (n) to |dW| <= rtol W, at most max_newton steps, then a bracketed Newton of
+ * at most max_bracket steps; P (5 x n) receives the primitives, iters (may be
+ * NULL) the total iterations (negative on failure), fallback (may be NULL) 1
+ * where the bracketed phase ran. No counterpart in the reference. */
+int vb_point_c2p_w(double gamma, const double* U, const double* W0, double rtol, int max_newton, int max_bracket,
+                   double* P, int* iters, int* fallback, int n, void* stream);
 
 #ifdef __cplusplus
 }

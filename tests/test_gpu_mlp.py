@@ -1,0 +1,124 @@
+"""GPU tests of the learned con2prim guess: the tensor-core forward and the
+gradients of the tensor-core training kernel against the CPU FP64 reference
+(oracle/mlp_ref.py), training convergence, the learned-guess solver against
+the plain FP64 path, and what the trained network gains over the method
+without it (Newton iterations from a cold start)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+G = 4.0 / 3.0
+
+
+def _features(m, n, seed=0, lorentz_max=100.0):
+    from verona_b200 import mlp
+
+    P = mlp.synthetic_states(n, G, seed=seed, lorentz_max=lorentz_max)
+    U = mlp.prim2con_torch(P, G)
+    return U, P
+
+
+def test_forward_matches_cpu_reference():
+    from oracle import mlp_ref
+    from verona_b200 import mlp
+
+    m = mlp.MLP(seed=3)
+    U, P = _features(m, 4096, seed=1)
+    m.fit_norm(U, G)
+    f, _ = m.features(U, P, G)
+    y = m.forward(f).cpu().numpy().astype(np.float64)
+    ref, _ = mlp_ref.forward(m.params(), f.cpu().numpy().astype(np.float64), bf=True)
+    rel = np.linalg.norm(y - ref) / np.linalg.norm(ref)
+    print("forward rel L2 error vs bf16-emulating reference:", rel, "max abs", np.max(np.abs(y - ref)))
+    assert rel < 1e-2
+
+
+def test_training_gradients_match_cpu_reference():
+    from oracle import mlp_ref
+    from verona_b200 import mlp
+
+    m = mlp.MLP(seed=5)
+    U, P = _features(m, 2048, seed=2)
+    m.fit_norm(U, G)
+    f, t = m.features(U, P, G)
+    loss = m.train_step(f, t, 0.0)  # lr = 0: gradients only
+    g_gpu = mlp_ref.split(m.grad())
+    l_ref, g_ref = mlp_ref.loss_and_grad(m.params(), f.cpu().numpy().astype(np.float64),
+                                         t.cpu().numpy().astype(np.float64))
+    g_ref = mlp_ref.split(g_ref)
+    assert abs(loss - l_ref) <= 2e-2 * l_ref
+    for k in ("W1", "b1", "W2", "b2", "W3", "b3", "w4", "b4"):
+        a, b = g_gpu[k].ravel(), g_ref[k].ravel()
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+        cos = float(a @ b / max(np.linalg.norm(a) * np.linalg.norm(b), 1e-30))
+        print(k, "rel", rel, "cos", cos)
+        assert rel < 5e-2 and cos > 0.998, (k, rel, cos)
+
+
+def test_training_converges():
+    from verona_b200 import mlp
+
+    m = mlp.MLP(seed=0)
+    hist = m.train(n_samples=1 << 18, epochs=4, batch=1 << 14, lr=3e-3, snapshots=False)
+    print("mse per epoch", hist)
+    assert hist[-1] < 0.05 * hist[0] and hist[-1] < 0.05
+
+
+@pytest.fixture(scope="module")
+def net():
+    from verona_b200 import mlp
+
+    m = mlp.MLP(seed=0)
+    m.train(n_samples=1 << 21, epochs=4, batch=1 << 15, lr=3e-3, snapshots=True)
+    return m
+
+
+def test_learned_guess_saves_newton_iterations(net):
+    """The judge is the bracketed W-Newton itself: from the network's guess
+    versus from a cold start (no previous state), on the training ranges."""
+    import torch
+
+    from verona_b200 import mlp
+
+    U, P = _features(net, 1 << 16, seed=99, lorentz_max=50.0)
+    f, _ = net.features(U, None, G)
+    y = net.forward(f).double()
+    p_guess = U[0] * torch.exp(y)
+    W_learned = p_guess - U[1]
+    W_cold = U[0] - U[1]  # D + E: the state-only start of the bracketed Newton
+    P_l, it_l, fb_l = mlp.c2p_w(U, W_learned, G)
+    P_c, it_c, fb_c = mlp.c2p_w(U, W_cold, G)
+    it_l, it_c = it_l.cpu().numpy(), it_c.cpu().numpy()
+    print("mean Newton iterations: learned %.2f, cold %.2f; fallbacks learned %d cold %d"
+          % (it_l.mean(), it_c.mean(), int(fb_l.sum()), int(fb_c.sum())))
+    assert (it_l > 0).all() and (it_c > 0).all()
+    assert it_l.mean() < 0.8 * it_c.mean()
+    # both refine to the same primitives
+    rel = ((P_l - P_c).abs() / (P_c.abs() + 1e-30))[0:2].max().item()
+    assert rel < 1e-9
+
+
+def test_learned_solver_matches_fp64_path(net):
+    from helpers import jet_ic, nozzle_params, per_field_rel
+    from verona_b200 import Solver
+
+    n = (32, 16, 24)
+    P0 = jet_ic(3, n, gamma=G, noise=0.03, seed=4)
+    dxs = [1.0 / 32] * 3
+    dt = 0.4 / sum(1.0 / d for d in dxs)
+    out = {}
+    for guess in ("previous", "learned"):
+        s = Solver(3, n, G, dxs, recon="wenoz", riemann="hllc", rk=3, guess=guess, n_iter=50, tol=1e-12, floor=1e-8,
+                   stats=1)
+        if guess == "learned":
+            net.attach(s)
+        s.set_boundary(0, 2, nozzle_params(3, n, 4.0, gamma=G))
+        s.load_prims(P0)
+        s.step(dt, 6)
+        out[guess] = (s.prims(), s.cons(), s.counters())
+    c = out["learned"][2]
+    print("learned counters", c.tolist(), "mean iterations", c[2] / max(c[3], 1))
+    assert c[0] == 0 and c[4] == 0
+    assert max(per_field_rel(out["learned"][1], out["previous"][1])) < 1e-9
+    assert max(per_field_rel(out["learned"][0], out["previous"][0])) < 1e-8

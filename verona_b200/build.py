@@ -65,7 +65,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     os.makedirs(OBJ, exist_ok=True)
     units = dict(UNITS)
     if os.path.exists(os.path.join(CSRC, "vb_mlp.cu")):
-        units["vb_mlp.cu"] = ["-fmad=true"]
+        units["vb_mlp.cu"] = ["-fmad=true"]  # the learned-guess Newton refinement is FP64 with FMA
     if os.path.exists(os.path.join(CSRC, "vb_batch.cu")):
         units["vb_batch.cu"] = ["-fmad=true"]
     if os.path.exists(os.path.join(CSRC, "vb_noalloc.cu")):

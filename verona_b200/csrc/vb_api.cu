@@ -22,6 +22,8 @@
 
 using namespace vb;
 
+extern "C" const void* vb_mlp_blob_ptr(vb_mlp_handle m);  // vb_mlp.cu
+
 struct vb_solver {
     int device = 0;
     int dims = 0, nv = 0, nghost = 3;
@@ -52,6 +54,9 @@ struct vb_solver {
     std::string err;
     // kernel variants
     vb_tuning tun{-1, 0, {0, 0, 0, 0, 0, 0}};
+    // learned con2prim guess
+    const void* mlp_blob = nullptr;
+    unsigned int* tc_err = nullptr;
     // profiling
     bool prof = false;
     std::vector<cudaEvent_t> ev;
@@ -138,6 +143,7 @@ int vb_destroy(vb_handle h) {
     cudaFree(h->cnt);
     cudaFree(h->partial);
     cudaFree(h->staging);
+    cudaFree(h->tc_err);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     cudaSetDevice(prev);
     delete h;
@@ -405,6 +411,11 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
     p.counters = h->cnt;
     p.force_box = h->tun.force_box;
     p.split = h->tun.split_con2prim < 0 ? default_split(h) : h->tun.split_con2prim;
+    p.skip_c2p = 0;
+    if (h->opt.guess == VB_GUESS_LEARNED) {
+        if (!h->mlp_blob) return fail(h, VB_ERR_STATE, "vb_step: guess = LEARNED needs vb_attach_mlp");
+        p.skip_c2p = 1;
+    }
     auto stage = [&](const R* Pin, R* Pout, const double* Us, double* Uo, double dts, double a, double b) -> int {
         for (int d = 0; d < 3; ++d) p.dtdx[d] = d < h->dims ? dts / h->dx[d] : 0.0;
         p.rk_a = a;
@@ -417,6 +428,10 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
             VB_CUDA(h, cudaEventRecord(e0, s));
         }
         VB_CUDA(h, launch_stage<R>(h->dims, h->opt.recon, h->opt.riemann, p, bufs, s));
+        if (p.skip_c2p) {
+            VB_CUDA(h, launch_c2p_learned(h->mlp_blob, p, Pin, Pout, fp32(h), Uo, h->tc_err, s));
+            h->launches += 1;
+        }
         if (h->prof) VB_CUDA(h, cudaEventRecord(e1, s));
         VB_CUDA(h, launch_ghost_limit<R>(g, Pin, Pout, h->opt.floor_, s));
         h->launches += 2 + (p.split && h->dims == 3 ? 1 : 0);
@@ -492,9 +507,12 @@ int vb_max_signal_speed(vb_handle h, double* c, void* stream) {
 int vb_get_counters(vb_handle h, uint64_t* out, int n, void* stream) {
     if (!h || !out || n < 0) return fail(h, VB_ERR_ARG, "vb_get_counters: bad argument");
     unsigned long long tmp[CNT_N];
+    unsigned int tce = 0;
     cudaStream_t s = (cudaStream_t)stream;
     VB_CUDA(h, cudaMemcpyAsync(tmp, h->cnt, sizeof tmp, cudaMemcpyDeviceToHost, s));
+    if (h->tc_err) VB_CUDA(h, cudaMemcpyAsync(&tce, h->tc_err, sizeof tce, cudaMemcpyDeviceToHost, s));
     VB_CUDA(h, cudaStreamSynchronize(s));
+    tmp[CNT_TIMEOUT] += tce ? 1 : 0;
     for (int i = 0; i < n; ++i) out[i] = i < CNT_N ? tmp[i] : 0;
     return VB_OK;
 }
@@ -527,6 +545,18 @@ int vb_profile_read(vb_handle h, double* stage_ms, int64_t* stage_launches, int6
     *all_launches = h->launches;
     h->ev_used = 0;
     h->launches = h->stage_launches = 0;
+    return VB_OK;
+}
+
+int vb_attach_mlp(vb_handle h, vb_mlp_handle m) {
+    if (!h || !m) return fail(h, VB_ERR_ARG, "vb_attach_mlp: null argument");
+    if (h->dims != 3 || h->nghost != 3) return fail(h, VB_ERR_UNSUPPORTED, "vb_attach_mlp: 3D grids only");
+    if (!h->tc_err) {
+        int rc = dev_alloc(h, (void**)&h->tc_err, sizeof(unsigned int));
+        if (rc) return rc;
+        VB_CUDA(h, cudaMemset(h->tc_err, 0, sizeof(unsigned int)));
+    }
+    h->mlp_blob = vb_mlp_blob_ptr(m);
     return VB_OK;
 }
 
@@ -569,6 +599,15 @@ int vb_point_con2prim(int dims, double gamma, int n_iter, double tol, const doub
     if (dims < 1 || dims > 3 || n_iter < 1 || !U || !P || n < 0)
         return fail(nullptr, VB_ERR_ARG, "vb_point_con2prim: bad argument");
     VB_CUDA(nullptr, launch_point_con2prim(dims, gamma, n_iter, tol, U, P, ret, n, (cudaStream_t)stream));
+    return VB_OK;
+}
+
+int vb_point_c2p_w(double gamma, const double* U, const double* W0, double rtol, int max_newton, int max_bracket,
+                   double* P, int* iters, int* fallback, int n, void* stream) {
+    if (!U || !W0 || !P || n < 0 || max_newton < 0 || max_bracket < 0 || !(rtol > 0))
+        return fail(nullptr, VB_ERR_ARG, "vb_point_c2p_w: bad argument");
+    VB_CUDA(nullptr, launch_point_c2p_w(gamma, U, W0, rtol, max_newton, max_bracket, P, iters, fallback, n,
+                                        (cudaStream_t)stream));
     return VB_OK;
 }
 

@@ -37,6 +37,7 @@ struct StageParams {
     unsigned long long* counters;
     int force_box;       // 1: use the box-tile kernel even where the z-marching one fits
     int split;           // 1: z-marching stencil kernel writes U only; k_c2p solves con2prim
+    int skip_c2p;        // 1: the stencil kernel writes U only and launches no con2prim
 };
 
 template <typename R> struct StageBufs {
@@ -89,11 +90,17 @@ cudaError_t launch_ref1d_store(const Ref1DState& st, double* P_aos, cudaStream_t
 
 int max_speed_blocks(const Grid& g);
 
+// learned-guess con2prim of a split stage (vb_mlp.cu)
+cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const void* Pin, void* Pout, bool fp32,
+                               const double* Uo, unsigned int* err, cudaStream_t s);
+
 // point kernels (FP64, vb_stage_f64.cu)
 cudaError_t launch_point_recon(int method, const double* q, double* out, int n, cudaStream_t s);
 cudaError_t launch_point_flux(int dims, int axis, int rs, double g, const double* PL, const double* PR, double* F,
                               int n, cudaStream_t s);
 cudaError_t launch_point_con2prim(int dims, double g, int n_iter, double tol, const double* U, double* P, int* ret,
                                   int n, cudaStream_t s);
+cudaError_t launch_point_c2p_w(double g, const double* U, const double* W0, double rtol, int max_newton,
+                               int max_bracket, double* P, int* iters, int* fallback, int n, cudaStream_t s);
 
 }  // namespace vb

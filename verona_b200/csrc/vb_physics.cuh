@@ -232,30 +232,60 @@ template <int DIM, typename T> VB_HD void harm_speeds(int d, T g, const T* P, T&
     lm = (v - r) / (T(1) + sig);
 }
 
+// Everything the Riemann solvers need from one face state, computed once:
+// conserved vector and flux along d (function_PtoU / function_PtoFx..z),
+// Lorentz factor, normal velocity, pressure and the HARM signal speeds
+// (src/3dim/algos.jl:117-157). Same expressions as the separate functions
+// above, so the values are identical.
+template <int DIM, typename T> struct FaceState {
+    static constexpr int NV = 2 + DIM;
+    T U[NV], F[NV];
+    T vn, p, lp, lm;
+    VB_HD void make(int d, T g, const T* P) {
+        T gam = lorentz<DIM>(P);
+        T w = g * P[1] + P[0];
+        T un = P[2 + d];
+        U[0] = gam * P[0];
+        U[1] = (g - T(1)) * P[1] - sq(gam) * w;
+        F[0] = P[0] * un;
+        F[1] = -w * un * gam;
+#pragma unroll
+        for (int m = 0; m < DIM; ++m) {
+            U[2 + m] = P[2 + m] * gam * w;
+            if (m == d)
+                F[2 + m] = sq(un) * w + (g - T(1)) * P[1];
+            else
+                F[2 + m] = P[2 + m] * un * w;
+        }
+        vn = un / gam;
+        p = (g - T(1)) * P[1];
+        T C = sound_speed(P[0], P[1], g);
+        T sig = sq(C) / (sq(gam) * (T(1) - sq(C)));
+        T r = sqrt(sig * (T(1) - sq(vn) + sig));
+        lp = (vn + r) / (T(1) + sig);
+        lm = (vn - r) / (T(1) + sig);
+    }
+};
+
 // HLL face flux, src/3dim/algos.jl:117-174 (states already floored)
 template <int DIM, typename T>
 VB_HD void hll_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
     constexpr int NV = 2 + DIM;
-    T UL[NV], UR[NV], FL[NV], FR[NV];
-    prim2con<DIM>(g, PR, UR);
-    prim2con<DIM>(g, PL, UL);
-    prim2flux<DIM>(d, g, PR, FR);
-    prim2flux<DIM>(d, g, PL, FL);
-    T lpL, lmL, lpR, lmR;
-    harm_speeds<DIM>(d, g, PL, lpL, lmL);
-    harm_speeds<DIM>(d, g, PR, lpR, lmR);
-    T Cmax = jmax(lpL, lpR);
-    T Cmin = -jmin(lmL, lmR);
+    FaceState<DIM, T> R, L;
+    R.make(d, g, PR);
+    L.make(d, g, PL);
+    T Cmax = jmax(L.lp, R.lp);
+    T Cmin = -jmin(L.lm, R.lm);
     if (Cmax < T(0)) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Fo[v] = FR[v];
+        for (int v = 0; v < NV; ++v) Fo[v] = R.F[v];
     } else if (Cmin < T(0)) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Fo[v] = FL[v];
+        for (int v = 0; v < NV; ++v) Fo[v] = L.F[v];
     } else {
 #pragma unroll
         for (int v = 0; v < NV; ++v)
-            Fo[v] = (FR[v] * Cmin + FL[v] * Cmax - Cmax * Cmin * (UR[v] - UL[v])) / (Cmax + Cmin);
+            Fo[v] = (R.F[v] * Cmin + L.F[v] * Cmax - Cmax * Cmin * (R.U[v] - L.U[v])) / (Cmax + Cmin);
     }
 }
 
@@ -266,32 +296,27 @@ VB_HD void hll_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
 template <int DIM, typename T>
 VB_HD void hllc_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
     constexpr int NV = 2 + DIM;
-    T UL[NV], UR[NV], FL[NV], FR[NV];
-    prim2con<DIM>(g, PR, UR);
-    prim2con<DIM>(g, PL, UL);
-    prim2flux<DIM>(d, g, PR, FR);
-    prim2flux<DIM>(d, g, PL, FL);
-    T lpL, lmL, lpR, lmR;
-    harm_speeds<DIM>(d, g, PL, lpL, lmL);
-    harm_speeds<DIM>(d, g, PR, lpR, lmR);
-    T Cmax = jmax(lpL, lpR);
-    T Cmin = -jmin(lmL, lmR);
+    FaceState<DIM, T> R, L;
+    R.make(d, g, PR);
+    L.make(d, g, PL);
+    T Cmax = jmax(L.lp, R.lp);
+    T Cmin = -jmin(L.lm, R.lm);
     if (Cmax < T(0)) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Fo[v] = FR[v];
+        for (int v = 0; v < NV; ++v) Fo[v] = R.F[v];
         return;
     }
     if (Cmin < T(0)) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Fo[v] = FL[v];
+        for (int v = 0; v < NV; ++v) Fo[v] = L.F[v];
         return;
     }
     T lL = -Cmin, lR = Cmax;
     T idl = T(1) / (lR - lL);
-    T E_L = -UL[1], E_R = -UR[1];
-    T m_L = UL[2 + d], m_R = UR[2 + d];
-    T FE_L = -FL[1], FE_R = -FR[1];
-    T Fm_L = FL[2 + d], Fm_R = FR[2 + d];
+    T E_L = -L.U[1], E_R = -R.U[1];
+    T m_L = L.U[2 + d], m_R = R.U[2 + d];
+    T FE_L = -L.F[1], FE_R = -R.F[1];
+    T Fm_L = L.F[2 + d], Fm_R = R.F[2 + d];
     T E_h = (lR * E_R - lL * E_L - (FE_R - FE_L)) * idl;
     T m_h = (lR * m_R - lL * m_L - (Fm_R - Fm_L)) * idl;
     T FE_h = (lR * FE_L - lL * FE_R + lR * lL * (E_R - E_L)) * idl;
@@ -305,17 +330,15 @@ VB_HD void hllc_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
     // selected one by one (no pointer to either side's arrays) so that every
     // array stays in registers
     const bool left = ls >= T(0);
-    T Pk[NV], U[NV], F[NV];
+    T U[NV], F[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        Pk[v] = left ? PL[v] : PR[v];
-        U[v] = left ? UL[v] : UR[v];
-        F[v] = left ? FL[v] : FR[v];
+        U[v] = left ? L.U[v] : R.U[v];
+        F[v] = left ? L.F[v] : R.F[v];
     }
     T lK = left ? lL : lR;
-    T lor = lorentz<DIM>(Pk);
-    T vn = Pk[2 + d] / lor;
-    T p = (g - T(1)) * Pk[1];
+    T vn = left ? L.vn : R.vn;
+    T p = left ? L.p : R.p;
     T E = -U[1];
     T fac = (lK - vn) / (lK - ls);
     T Us[NV];

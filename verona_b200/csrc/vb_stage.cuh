@@ -203,6 +203,7 @@ __global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
             b.Uo[v * vs + gidx] = u;
             P[v] = (double)b.Pin[v * vs + gidx];
         }
+        if (p.skip_c2p) continue;  // con2prim runs in a separate kernel
         int fb;
         int r = solve_cell<DIM>(p, U, P, gidx, fb);
         n_fail += (r < 0);
@@ -243,6 +244,8 @@ cudaError_t launch_stage_t(const StageParams& p, const StageBufs<R>& b, cudaStre
     cudaGetDevice(&dev);
     if (!(attr_set >> (dev & 63) & 1ULL)) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         attr_set |= 1ULL << (dev & 63);
     }

@@ -79,6 +79,28 @@ cudaError_t launch_point_con2prim(int dims, double g, int n_iter, double tol, co
     return cudaGetLastError();
 }
 
+// Newton on W from given guesses (the learned path's refinement), FP64
+__global__ void k_point_c2p_w(double g, const double* __restrict__ U, const double* __restrict__ W0, double rtol,
+                              int max_newton, int max_bracket, double* __restrict__ P, int* __restrict__ iters,
+                              int* __restrict__ fallback, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double u[5], p[5];
+        for (int v = 0; v < 5; ++v) u[v] = U[v * n + i];
+        int fb = 0;
+        int r = c2p_w(g, u, W0[i], rtol, max_newton, max_bracket, p, &fb);
+        for (int v = 0; v < 5; ++v) P[v * n + i] = p[v];
+        if (iters) iters[i] = r;
+        if (fallback) fallback[i] = fb;
+    }
+}
+
+cudaError_t launch_point_c2p_w(double g, const double* U, const double* W0, double rtol, int max_newton,
+                               int max_bracket, double* P, int* iters, int* fallback, int n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_point_c2p_w<<<grid_for(n, 128), 128, 0, s>>>(g, U, W0, rtol, max_newton, max_bracket, P, iters, fallback, n);
+    return cudaGetLastError();
+}
+
 int max_speed_blocks(const Grid& g) {
     (void)g;
     return 148 * 4;

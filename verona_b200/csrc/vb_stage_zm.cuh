@@ -393,12 +393,14 @@ cudaError_t launch_stage_zm_t(const StageParams& p, const StageBufs<R>& b, cudaS
     if (!(attr_set >> (dev & 63) & 1ULL)) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
         attr_set |= 1ULL << (dev & 63);
     }
     dim3 grid((p.n[0] - 2 * NG) / C::TX, (p.n[1] - 2 * NG) / C::TY, (p.n[2] - 2 * NG + C::LZ - 1) / C::LZ);
     kern<<<grid, C::TX * C::TY, smem, s>>>(p, b);
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess || !SPLIT) return e;
+    if (e != cudaSuccess || !SPLIT || p.skip_c2p) return e;
     const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
     k_c2p<R><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
     return cudaGetLastError();
@@ -406,7 +408,8 @@ cudaError_t launch_stage_zm_t(const StageParams& p, const StageBufs<R>& b, cudaS
 
 template <int REC, int RS, typename R>
 cudaError_t launch_stage_zm(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
-    return p.split ? launch_stage_zm_t<REC, RS, R, true>(p, b, s) : launch_stage_zm_t<REC, RS, R, false>(p, b, s);
+    return (p.split || p.skip_c2p) ? launch_stage_zm_t<REC, RS, R, true>(p, b, s)
+                                   : launch_stage_zm_t<REC, RS, R, false>(p, b, s);
 }
 
 template <typename R>
