@@ -206,18 +206,21 @@ int vb_mlp_param_count(void);
 /* host arrays: params[vb_mlp_param_count()], norm[8] */
 int vb_mlp_set_params(vb_mlp_handle m, const float* params, const float* norm, void* stream);
 int vb_mlp_get_params(vb_mlp_handle m, float* params, float* norm, void* stream);
-/* features (n x 4) and, if P != NULL, targets log(p/D) (n) of n conserved states U
- * (5 x n, FP64 struct-of-arrays; P likewise) */
+/* features (n x 4) and, if P != NULL, targets log(p/D) (n) and loss weights
+ * max((p/W)^2, 1e-4) (n; may be NULL) of n conserved states U (5 x n, FP64
+ * struct-of-arrays; P likewise). The weight is the sensitivity of the Newton
+ * start W0 = E + p to log p: cold flows, whose p is ill-conditioned in U,
+ * weigh little. */
 int vb_mlp_features(vb_mlp_handle m, const double* U, const double* P, int n, double gamma, float* feat,
-                    float* target, void* stream);
+                    float* target, float* weight, void* stream);
 /* tensor-core inference: out[n] = y(feat) */
 int vb_mlp_forward(vb_mlp_handle m, const float* feat, int n, float* out, void* stream);
-/* one optimisation step on n samples (mean squared error on y): forward and
- * backward on the tensor cores, then Adam with learning rate lr (lr = 0:
- * gradients only); *loss (may be NULL) receives the batch loss. Synchronises
- * when loss != NULL. */
-int vb_mlp_train_step(vb_mlp_handle m, const float* feat, const float* target, int n, float lr, float* loss,
-                      void* stream);
+/* one optimisation step on n samples (weighted mean squared error on y,
+ * weight may be NULL): forward and backward on the tensor cores, then Adam
+ * with learning rate lr (lr = 0: gradients only); *loss (may be NULL)
+ * receives the batch loss. Synchronises when loss != NULL. */
+int vb_mlp_train_step(vb_mlp_handle m, const float* feat, const float* target, const float* weight, int n, float lr,
+                      float* loss, void* stream);
 /* host copy of the gradient of the last step (same layout as the parameters) */
 int vb_mlp_get_grad(vb_mlp_handle m, float* grad, void* stream);
 /* use the network as the con2prim guess of a 3D solver (options.guess =

@@ -120,9 +120,12 @@ __global__ void k_mlp_pack(const float* __restrict__ prm, const float* __restric
     }
 }
 
-// features and targets y = log(p / D) of n states (U: 5 x n SoA FP64, P: 5 x n)
+// features, targets y = log(p / D) and loss weights (p / W)^2 -- the
+// sensitivity of the Newton start W0 = E + p to log p -- of n states
+// (U, P: 5 x n SoA FP64)
 __global__ void k_mlp_features(const double* __restrict__ U, const double* __restrict__ P, int n, double gamma,
-                               const float* __restrict__ norm, float* __restrict__ feat, float* __restrict__ target) {
+                               const float* __restrict__ norm, float* __restrict__ feat, float* __restrict__ target,
+                               float* __restrict__ weight) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double u[5];
         for (int v = 0; v < 5; ++v) u[v] = U[v * (long long)n + i];
@@ -133,6 +136,11 @@ __global__ void k_mlp_features(const double* __restrict__ U, const double* __res
         if (P && target) {
             double p = (gamma - 1.0) * P[1 * (long long)n + i];
             target[i] = (float)(log(fmax(p, 1e-300)) - ld);
+            if (weight) {
+                double W = p - u[1];
+                double r = p / W;
+                weight[i] = (float)fmax(r * r, 1e-4);
+            }
         }
     }
 }
@@ -436,9 +444,9 @@ __device__ __forceinline__ bool run_mma(TrainSmem& s, uint32_t& phase, unsigned 
 }
 
 __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict__ blob, const float* __restrict__ feat,
-                                                       const float* __restrict__ target, int n, float inv_batch,
-                                                       float* __restrict__ grad, float* __restrict__ loss_out,
-                                                       unsigned int* err) {
+                                                       const float* __restrict__ target, const float* __restrict__ weight,
+                                                       int n, float inv_batch, float* __restrict__ grad,
+                                                       float* __restrict__ loss_out, unsigned int* err) {
     extern __shared__ __align__(128) unsigned char smraw[];
     TrainSmem& s = *reinterpret_cast<TrainSmem*>(smraw);
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -484,10 +492,11 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict
     for (int tile = blockIdx.x; tile < ntiles && good; tile += gridDim.x) {
         const int i = tile * TILE + t;
         const bool ok = i < n;
-        float x[4] = {0.f, 0.f, 0.f, 0.f}, tgt = 0.f;
+        float x[4] = {0.f, 0.f, 0.f, 0.f}, tgt = 0.f, wgt = 0.f;
         if (ok) {
             for (int k = 0; k < 4; ++k) x[k] = feat[i * 4 + k];
             tgt = target[i];
+            wgt = weight ? weight[i] : 1.0f;
         }
         float z[64], g[64];
         // ---- forward ----
@@ -524,8 +533,8 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict
             y = fmaf(s.w4[k], g[k], y);
         }
         const float r = ok ? (y - tgt) : 0.0f;
-        loss += r * r;
-        const float dy = 2.0f * r * inv_batch;
+        loss += wgt * r * r;
+        const float dy = 2.0f * wgt * r * inv_batch;
         // ---- layer 4 gradients: [h3^T; 1] x dy^T ----
 #pragma unroll
         for (int k = 0; k < 64; ++k) st_bf16(s.at, TILE, k, t, ok ? g[k] : 0.0f);
@@ -812,11 +821,12 @@ int vb_mlp_get_params(vb_mlp_handle m, float* params, float* norm, void* stream)
 }
 
 int vb_mlp_features(vb_mlp_handle m, const double* U, const double* P, int n, double gamma, float* feat,
-                    float* target, void* stream) {
+                    float* target, float* weight, void* stream) {
     if (!m || !U || !feat || n < 0) return mfail(m, VB_ERR_ARG, "vb_mlp_features: bad argument");
     if (n == 0) return VB_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    k_mlp_features<<<std::min((n + 255) / 256, 148 * 16), 256, 0, s>>>(U, P, n, gamma, m->norm, feat, target);
+    k_mlp_features<<<std::min((n + 255) / 256, 148 * 16), 256, 0, s>>>(U, P, n, gamma, m->norm, feat, target,
+                                                                        weight);
     MCUDA(m, cudaGetLastError());
     return VB_OK;
 }
@@ -832,16 +842,16 @@ int vb_mlp_forward(vb_mlp_handle m, const float* feat, int n, float* out, void* 
     return mlp_check_err(m, s);
 }
 
-int vb_mlp_train_step(vb_mlp_handle m, const float* feat, const float* target, int n, float lr, float* loss,
-                      void* stream) {
+int vb_mlp_train_step(vb_mlp_handle m, const float* feat, const float* target, const float* weight, int n, float lr,
+                      float* loss, void* stream) {
     if (!m || !feat || !target || n <= 0 || !(lr >= 0.0f)) return mfail(m, VB_ERR_ARG, "vb_mlp_train_step: bad argument");
     cudaStream_t s = (cudaStream_t)stream;
     MCUDA(m, cudaMemsetAsync(m->grad, 0, sizeof(float) * N_PARAMS, s));
     MCUDA(m, cudaMemsetAsync(m->loss, 0, sizeof(float), s));
     MCUDA(m, cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem)));
     int tiles = (n + TILE - 1) / TILE;
-    k_mlp_train<<<std::min(tiles, 148), TILE, sizeof(TrainSmem), s>>>(m->blob, feat, target, n, 1.0f / (float)n,
-                                                                       m->grad, m->loss, m->err);
+    k_mlp_train<<<std::min(tiles, 148), TILE, sizeof(TrainSmem), s>>>(m->blob, feat, target, weight, n,
+                                                                       1.0f / (float)n, m->grad, m->loss, m->err);
     MCUDA(m, cudaGetLastError());
     if (lr > 0.0f) {
         m->adam_t += 1;

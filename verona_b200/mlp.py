@@ -37,9 +37,9 @@ def _sig():
         "vb_mlp_param_count": [],
         "vb_mlp_set_params": [vp, fp, fp, vp],
         "vb_mlp_get_params": [vp, fp, fp, vp],
-        "vb_mlp_features": [vp, vp, vp, C.c_int, C.c_double, vp, vp, vp],
+        "vb_mlp_features": [vp, vp, vp, C.c_int, C.c_double, vp, vp, vp, vp],
         "vb_mlp_forward": [vp, vp, C.c_int, vp, vp],
-        "vb_mlp_train_step": [vp, vp, vp, C.c_int, C.c_float, fp, vp],
+        "vb_mlp_train_step": [vp, vp, vp, vp, C.c_int, C.c_float, fp, vp],
         "vb_mlp_get_grad": [vp, fp, vp],
         "vb_attach_mlp": [vp, vp],
         "vb_point_c2p_w": [C.c_double, vp, vp, C.c_double, C.c_int, C.c_int, vp, vp, vp, C.c_int, vp],
@@ -197,16 +197,18 @@ class MLP:
         _chk(self.lib.vb_mlp_get_grad(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), None), self._h)
         return out
 
-    def features(self, U, P=None, gamma=4.0 / 3.0):
-        """U, P: (5, n) FP64 CUDA tensors -> (feat (n, 4), target (n,) or None)."""
+    def features(self, U, P=None, gamma=4.0 / 3.0, with_weight=False):
+        """U, P: (5, n) FP64 CUDA tensors -> (feat (n, 4), target (n,) or None[, weight (n,)])."""
         import torch
 
         n = U.shape[1]
         feat = torch.empty((n, 4), dtype=torch.float32, device="cuda")
         tgt = torch.empty(n, dtype=torch.float32, device="cuda") if P is not None else None
+        wgt = torch.empty(n, dtype=torch.float32, device="cuda") if (P is not None and with_weight) else None
         _chk(self.lib.vb_mlp_features(self._h, _ptr(U.contiguous()), _ptr(P.contiguous()) if P is not None else None,
-                                      n, gamma, _ptr(feat), _ptr(tgt) if tgt is not None else None, None), self._h)
-        return feat, tgt
+                                      n, gamma, _ptr(feat), _ptr(tgt) if tgt is not None else None,
+                                      _ptr(wgt) if wgt is not None else None, None), self._h)
+        return (feat, tgt, wgt) if with_weight else (feat, tgt)
 
     def forward(self, feat):
         import torch
@@ -216,10 +218,10 @@ class MLP:
         _chk(self.lib.vb_mlp_forward(self._h, _ptr(feat.contiguous()), n, _ptr(out), None), self._h)
         return out
 
-    def train_step(self, feat, target, lr):
+    def train_step(self, feat, target, lr, weight=None):
         loss = C.c_float()
-        _chk(self.lib.vb_mlp_train_step(self._h, _ptr(feat), _ptr(target), feat.shape[0], float(lr), C.byref(loss),
-                                        None), self._h)
+        _chk(self.lib.vb_mlp_train_step(self._h, _ptr(feat), _ptr(target), _ptr(weight) if weight is not None else None,
+                                        feat.shape[0], float(lr), C.byref(loss), None), self._h)
         return loss.value
 
     def fit_norm(self, U, gamma):
@@ -236,7 +238,7 @@ class MLP:
         self.set_params(self.params(), self.norm)
         del torch
 
-    def train(self, n_samples=1 << 22, gammas=(4.0 / 3.0, 5.0 / 3.0), epochs=6, batch=1 << 16, lr=3e-3, seed=0,
+    def train(self, n_samples=1 << 22, gammas=(4.0 / 3.0, 5.0 / 3.0), epochs=4, batch=1 << 12, lr=3e-3, seed=0,
               snapshots=True, log=None):
         """Train on synthetic states (+ solver snapshots); returns the loss history per epoch."""
         import torch
@@ -252,14 +254,24 @@ class MLP:
         # normalisation from the first gamma's states, then features of every set
         self.fit_norm(prim2con_torch(Ps[0][0], Ps[0][1]), Ps[0][1])
         del allU
+        wgts = []
         for P, g in Ps:
-            f, t = self.features(prim2con_torch(P, g), P, g)
-            ok = torch.isfinite(t) & torch.isfinite(f).all(1)
+            f, t, w = self.features(prim2con_torch(P, g), P, g, with_weight=True)
+            ok = torch.isfinite(t) & torch.isfinite(f).all(1) & torch.isfinite(w)
             feats.append(f[ok])
             tgts.append(t[ok])
+            wgts.append(w[ok])
         F = torch.cat(feats)
         T = torch.cat(tgts)
+        Wt = torch.cat(wgts)
         n = F.shape[0]
+        # start the output layer at the target's mean and scale
+        prm = split_params(self.params())
+        tm = float((T * Wt).sum() / Wt.sum())
+        ts = float(torch.sqrt(((T - tm) ** 2 * Wt).sum() / Wt.sum()))
+        prm["b4"][:] = tm
+        prm["w4"][:] = prm["w4"] * ts
+        self.set_params(np.concatenate([prm[k].ravel() for k in ("W1", "b1", "W2", "b2", "W3", "b3", "w4", "b4")]))
         gen = torch.Generator(device="cuda")
         gen.manual_seed(seed)
         hist = []
@@ -273,7 +285,7 @@ class MLP:
                 idx = perm[b0:b0 + batch]
                 # cosine learning-rate schedule
                 lr_t = lr * 0.5 * (1 + math.cos(math.pi * step / total_steps))
-                tot += self.train_step(F[idx].contiguous(), T[idx].contiguous(), lr_t)
+                tot += self.train_step(F[idx].contiguous(), T[idx].contiguous(), lr_t, Wt[idx].contiguous())
                 nb += 1
                 step += 1
             hist.append(tot / max(nb, 1))
