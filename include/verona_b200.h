@@ -193,9 +193,10 @@ int vb_point_con2prim(int dims, double gamma, int n_iter, double tol, const doub
 /* ---- learned con2prim guess (extension; the reference warm-starts Newton from
  * the previous primitive state, src/3dim/structs.jl:277-287) ----------------------
  * A 4 -> 64 -> 64 -> 64 -> 1 SiLU MLP in BF16 on the tensor cores (tcgen05, FP32
- * accumulation in TMEM). Features f = (log D, log1p(|S|/D), log max(tau/D, 1e-12),
- * Gamma) normalised by norm = {mean[4], 1/std[4]}; output y = log(p/D). Parameters
- * are one FP32 vector of vb_mlp_param_count() values:
+ * accumulation in TMEM). With E = tau + D = -U2: features f = (log D, |S|/E,
+ * log(E/D), Gamma) normalised by norm = {mean[4], 1/std[4]}; output y, the
+ * pressure guess as a fraction of E: p0 = E max(y, 0), Newton start
+ * W0 = E + p0. Parameters are one FP32 vector of vb_mlp_param_count() values:
  * W1[4][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] w4[64] b4 (W[in][out]).
  * All array arguments are device pointers. */
 typedef struct vb_mlp* vb_mlp_handle;
@@ -206,11 +207,10 @@ int vb_mlp_param_count(void);
 /* host arrays: params[vb_mlp_param_count()], norm[8] */
 int vb_mlp_set_params(vb_mlp_handle m, const float* params, const float* norm, void* stream);
 int vb_mlp_get_params(vb_mlp_handle m, float* params, float* norm, void* stream);
-/* features (n x 4) and, if P != NULL, targets log(p/D) (n) and loss weights
- * max((p/W)^2, 1e-4) (n; may be NULL) of n conserved states U (5 x n, FP64
- * struct-of-arrays; P likewise). The weight is the sensitivity of the Newton
- * start W0 = E + p to log p: cold flows, whose p is ill-conditioned in U,
- * weigh little. */
+/* features (n x 4) and, if P != NULL, targets x = p/E (n) and loss weights
+ * 1/(1+x)^2 (n; may be NULL) of n conserved states U (5 x n, FP64
+ * struct-of-arrays; P likewise): the weighted squared error of y is the
+ * squared relative error of the Newton start W0. */
 int vb_mlp_features(vb_mlp_handle m, const double* U, const double* P, int n, double gamma, float* feat,
                     float* target, float* weight, void* stream);
 /* tensor-core inference: out[n] = y(feat) */

@@ -57,12 +57,22 @@ def test_training_gradients_match_cpu_reference():
 
 
 def test_training_converges():
+    """Weighted MSE on held-out states, before and after training."""
     from verona_b200 import mlp
 
     m = mlp.MLP(seed=0)
+    U, P = _features(m, 1 << 15, seed=77)
+    m.fit_norm(U, G)
+
+    def held_out_loss():
+        f, t, w = m.features(U, P, G, with_weight=True)
+        return m.train_step(f, t, 0.0, w)
+
+    before = held_out_loss()
     hist = m.train(n_samples=1 << 18, epochs=6, batch=1 << 12, lr=3e-3, snapshots=False)
-    print("weighted mse per epoch", hist)
-    assert hist[-1] < 0.2 * hist[0]
+    after = held_out_loss()
+    print("held-out weighted mse: before %.3e after %.3e; per epoch %s" % (before, after, hist))
+    assert after < 0.05 * before and after < 1e-2
 
 
 @pytest.fixture(scope="module")
@@ -84,9 +94,12 @@ def test_learned_guess_saves_newton_iterations(net):
     U, P = _features(net, 1 << 16, seed=99, lorentz_max=50.0)
     f, _ = net.features(U, None, G)
     y = net.forward(f).double()
-    p_guess = U[0] * torch.exp(y)
-    W_learned = p_guess - U[1]
+    assert torch.isfinite(y).all()
+    W_learned = -U[1] * (1 + y.clamp(min=0))
     W_cold = U[0] - U[1]  # D + E: the state-only start of the bracketed Newton
+    W_true = (G - 1) * P[1] - U[1]
+    err = ((W_learned - W_true) / W_true).abs()
+    print("learned W0 relative error: median %.2e, 99%% %.2e" % (err.median().item(), err.quantile(0.99).item()))
     P_l, it_l, fb_l = mlp.c2p_w(U, W_learned, G)
     P_c, it_c, fb_c = mlp.c2p_w(U, W_cold, G)
     it_l, it_c = it_l.cpu().numpy(), it_c.cpu().numpy()

@@ -1,12 +1,16 @@
 // Learned con2prim initial guess: a 4 -> 64 -> 64 -> 64 -> 1 SiLU MLP in
 // BF16 on the sm_100a tensor cores (tcgen05, FP32 accumulation in TMEM).
 //
-// Inputs per cell (the conserved state only): f = (log D, log1p(|S|/D),
-// log max(tau/D, 1e-12), Gamma_eos) with tau = -U2 - D, normalised by the
+// Inputs per cell (the conserved state only), with E = tau + D = -U2 the
+// total energy: f = (log D, |S|/E, log(E/D), Gamma_eos), normalised by the
 // training-set mean and standard deviation. The network predicts
-// y = log(p / D); the guess is log p = y + log D and W0 = p - U2
-// (U2 = T^t_t = p - W). Newton on W then refines the guess to the requested
-// relative tolerance, with a bracketed fallback (vb_con2prim.cuh, c2p_w).
+// x = p / E (in [0, Gamma - 1) for physical states); the pressure guess is
+// p0 = E max(y, 0) and the Newton start W0 = E + p0 = E (1 + max(y, 0))
+// (U2 = T^t_t = p - W). Training minimises ((y - x) / (1 + x))^2, the squared
+// relative error of W0. (log p itself is ill-conditioned in U for cold
+// relativistic flows, where p sits below the precision of E.) Newton on W
+// then refines the guess to the requested relative tolerance, with a
+// bracketed fallback (vb_con2prim.cuh, c2p_w).
 //
 // Kernels
 //   k_mlp_pack      FP32 master parameters -> BF16 operand blobs in the
@@ -75,10 +79,10 @@ __device__ __forceinline__ void cell_features(const double* U, double gamma, con
                                               float* f, double* logD) {
     const double D = U[0];
     const double S = sqrt(U[2] * U[2] + U[3] * U[3] + U[4] * U[4]);
-    const double tau = -U[1] - D;
+    const double E = -U[1];
     const double ld = log(fmax(D, 1e-300));
     *logD = ld;
-    float raw[4] = {(float)ld, (float)log1p(S / D), (float)log(fmax(tau / D, 1e-12)), (float)gamma};
+    float raw[4] = {(float)ld, (float)(S / E), (float)log(fmax(E / D, 1e-300)), (float)gamma};
 #pragma unroll
     for (int i = 0; i < 4; ++i) f[i] = (raw[i] - mu[i]) * isd[i];
 }
@@ -120,8 +124,8 @@ __global__ void k_mlp_pack(const float* __restrict__ prm, const float* __restric
     }
 }
 
-// features, targets y = log(p / D) and loss weights (p / W)^2 -- the
-// sensitivity of the Newton start W0 = E + p to log p -- of n states
+// features, targets x = p / E and loss weights 1 / (1 + x)^2 (so the
+// weighted squared error is that of W0 relative to W) of n states
 // (U, P: 5 x n SoA FP64)
 __global__ void k_mlp_features(const double* __restrict__ U, const double* __restrict__ P, int n, double gamma,
                                const float* __restrict__ norm, float* __restrict__ feat, float* __restrict__ target,
@@ -134,13 +138,10 @@ __global__ void k_mlp_features(const double* __restrict__ U, const double* __res
         cell_features(u, gamma, norm, norm + MLP_IN, f, &ld);
         for (int k = 0; k < 4; ++k) feat[i * 4 + k] = f[k];
         if (P && target) {
-            double p = (gamma - 1.0) * P[1 * (long long)n + i];
-            target[i] = (float)(log(fmax(p, 1e-300)) - ld);
-            if (weight) {
-                double W = p - u[1];
-                double r = p / W;
-                weight[i] = (float)fmax(r * r, 1e-4);
-            }
+            const double p = (gamma - 1.0) * P[1 * (long long)n + i];
+            const double x = p / (-u[1]);
+            target[i] = (float)x;
+            if (weight) weight[i] = (float)(1.0 / ((1.0 + x) * (1.0 + x)));
         }
     }
 }
@@ -357,8 +358,7 @@ __global__ void __launch_bounds__(TILE) k_c2p_learned(const MlpBlob* __restrict_
         float y = 0.f;
         if (!mlp_forward_tile(s, f, y, phase, a.err)) break;
         if (!ok) continue;
-        const double p0 = exp(ld + (double)y);
-        const double W0 = p0 - U[1];
+        const double W0 = -U[1] * (1.0 + fmax((double)y, 0.0));
         double P[5];
         int fb;
         int r = c2p_w(a.gamma, U, W0, a.rtol, a.max_newton, a.max_bracket, P, &fb);

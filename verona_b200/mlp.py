@@ -1,8 +1,9 @@
 """Learned con2prim initial guess: training data, training loop and use.
 
 The network (4 -> 64 -> 64 -> 64 -> 1, SiLU, BF16 on the tensor cores with
-FP32 accumulation; vb_mlp.cu) maps a conserved state to y = log(p / D). Its
-training pairs are conserved/primitive pairs made by the solver itself:
+FP32 accumulation; vb_mlp.cu) maps a conserved state to the pressure guess
+as a fraction of the total energy E = tau + D, y ~ p / E; Newton on
+W = rho h gamma^2 starts from W0 = E (1 + max(y, 0)). Its training pairs are conserved/primitive pairs made by the solver itself:
   * synthetic states with log-uniform rho in [1e-4, 10], log-uniform p/rho in
     [1e-6, 1e2], log-uniform Lorentz factor in [1, 100] in a random direction
     and Gamma in {4/3, 5/3};
