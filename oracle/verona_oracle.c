@@ -266,7 +266,8 @@ static void hll_flux(int dims, int d, double g, const double* PL, const double* 
 
 /* HLLC face flux (extension; not in the reference, which is HLL only).
  * Mignone & Bodo (2005, MNRAS 364, 126) SRHD HLLC with the same HARM/Davis
- * speed estimates as the reference HLL. Verona's conserved vector is
+ * speed estimates as the reference HLL, falling back to HLL where the star
+ * state is unphysical (p* <= 0, contact outside [lambda_L, lambda_R]). Verona's conserved vector is
  * (D, -E, m_1..m_dims) and its flux (D v, -m_n, m v + p e_n). */
 static void hllc_flux(int dims, int d, double g, const double* PL, const double* PR, double* Fo) {
     int nv = 2 + dims;
@@ -305,6 +306,12 @@ static void hllc_flux(int dims, int d, double g, const double* PL, const double*
     if (disc < 0.0) disc = 0.0;
     double ls = 2.0 * m_h / (b + sqrt(disc));
     double ps = Fm_h - FE_h * ls;
+    /* unphysical star state: the HLL flux of the same states */
+    if (!(ps > 0.0) || !(ls >= lL && ls <= lR)) {
+        for (int v = 0; v < nv; ++v)
+            Fo[v] = (FR[v] * Cmin + FL[v] * Cmax - Cmax * Cmin * (UR[v] - UL[v])) / (Cmax + Cmin);
+        return;
+    }
     const double* P;
     const double* U;
     const double* F;

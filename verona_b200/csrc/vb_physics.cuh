@@ -291,8 +291,8 @@ VB_HD void hll_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
 
 // HLLC face flux: an extension (the reference is HLL only). Mignone & Bodo
 // (2005, MNRAS 364, 126) relativistic HLLC with the HARM/Davis speed bounds
-// of the HLL above. Verona's conserved vector is (D, -E, m) and its flux
-// (D v_n, -m_n, m v_n + p e_n).
+// of the HLL above, falling back to HLL where the star state is unphysical.
+// Verona's conserved vector is (D, -E, m) and its flux (D v_n, -m_n, m v_n + p e_n).
 template <int DIM, typename T>
 VB_HD void hllc_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
     constexpr int NV = 2 + DIM;
@@ -326,6 +326,14 @@ VB_HD void hllc_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
     if (disc < T(0)) disc = T(0);
     T ls = T(2) * m_h / (b + sqrt(disc));
     T ps = Fm_h - FE_h * ls;
+    // unphysical star state (negative pressure, contact outside the fan, not
+    // finite): fall back to the HLL flux of the same states
+    if (!(ps > T(0)) || !(ls >= lL && ls <= lR)) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+            Fo[v] = (R.F[v] * Cmin + L.F[v] * Cmax - Cmax * Cmin * (R.U[v] - L.U[v])) / (Cmax + Cmin);
+        return;
+    }
     // star state of the side the contact leaves behind x/t = 0; values are
     // selected one by one (no pointer to either side's arrays) so that every
     // array stays in registers

@@ -163,6 +163,9 @@ def solver_snapshots(gamma: float, max_states: int = 1 << 20):
         out.append(q)
     s.close()
     Q = np.concatenate(out, axis=1)
+    # keep physical states only (a run may leave NaN cells where its con2prim failed)
+    good = np.isfinite(Q).all(0) & (Q[0] > 0) & (Q[1] > 0)
+    Q = Q[:, good]
     if Q.shape[1] > max_states:
         Q = Q[:, np.random.default_rng(0).choice(Q.shape[1], max_states, replace=False)]
     return torch.from_numpy(np.ascontiguousarray(Q)).cuda()
@@ -232,6 +235,9 @@ class MLP:
         self.norm = np.array([0, 0, 0, 0, 1, 1, 1, 1], dtype=np.float32)
         self.set_params(self.params(), self.norm)
         raw, _ = self.features(U, None, gamma)
+        raw = raw[torch.isfinite(raw).all(1)]
+        if raw.shape[0] < 16:
+            raise ValueError("fit_norm: fewer than 16 states with finite features")
         mu = raw.mean(0).double().cpu().numpy()
         sd = raw.std(0).double().cpu().numpy()
         sd = np.where(sd > 1e-6, sd, 1.0)
@@ -266,6 +272,8 @@ class MLP:
         T = torch.cat(tgts)
         Wt = torch.cat(wgts)
         n = F.shape[0]
+        if n < batch:
+            raise ValueError(f"train: only {n} usable samples for batch {batch}")
         # start the output layer at the target's mean and scale
         prm = split_params(self.params())
         tm = float((T * Wt).sum() / Wt.sum())
