@@ -85,7 +85,7 @@ def net():
 
 
 def test_learned_guess_saves_newton_iterations(net):
-    """The judge is the bracketed W-Newton itself: from the network's guess
+    """Measured by the bracketed W-Newton itself: from the network's guess
     versus from a cold start (no previous state), on the training ranges."""
     import torch
 
@@ -105,11 +105,23 @@ def test_learned_guess_saves_newton_iterations(net):
     it_l, it_c = it_l.cpu().numpy(), it_c.cpu().numpy()
     print("mean Newton iterations: learned %.2f, cold %.2f; fallbacks learned %d cold %d"
           % (it_l.mean(), it_c.mean(), int(fb_l.sum()), int(fb_c.sum())))
-    assert (it_l > 0).all() and (it_c > 0).all()
-    assert it_l.mean() < 0.8 * it_c.mean()
-    # both refine to the same primitives
-    rel = ((P_l - P_c).abs() / (P_c.abs() + 1e-30))[0:2].max().item()
-    assert rel < 1e-9
+    print("failed solves: learned %d, cold %d" % (int((it_l <= 0).sum()), int((it_c <= 0).sum())))
+    assert (it_l > 0).all()
+    ok = it_c > 0
+    assert it_l[ok].mean() < 0.8 * it_c[ok].mean()
+    # both refine to the same state where both converge. W (the Newton
+    # unknown) stops at a step of rtol 1e-12; the density D / Lorentz and the
+    # spatial four-velocity (relative to the Lorentz factor) inherit that error
+    # amplified by about Lorentz^2 through Lorentz(W), and the internal
+    # energy follows from W by a cancellation when p << W and is floored at
+    # 1e-8, so it is compared to W plus that floor
+    okt = torch.from_numpy(ok).cuda()
+    Pl, Pc = P_l[:, okt], P_c[:, okt]
+    lor = torch.sqrt(1 + Pc[2] ** 2 + Pc[3] ** 2 + Pc[4] ** 2)
+    W = (Pc[0] + G * Pc[1]) * lor**2
+    assert ((Pl[0] - Pc[0]).abs() / Pc[0] / (1e-11 * lor**2)).max().item() < 1.0
+    assert ((Pl[2:5] - Pc[2:5]).abs() / lor / (1e-11 * lor**2)).max().item() < 1.0
+    assert ((Pl[1] - Pc[1]).abs() / (1e-10 * W + 2e-8)).max().item() < 1.0
 
 
 def test_learned_solver_matches_fp64_path(net):

@@ -71,9 +71,14 @@ VB_HD int c2p_1d(double g, int n_iter, double tol, const double* U, double* P) {
 // singular matrix (the reference raises an error there).
 VB_HD bool lu_pivot4(double* A, double* t, double* x) {
 #define I4(i, j) (((j)-1) * 4 + (i)-1)
+    // every loop is unrolled and the pivot row swap is a predicated swap with
+    // each candidate row, so all indices are compile-time and A, t, rn stay
+    // in registers
     double rn[4];
+#pragma unroll
     for (int i = 1; i <= 4; ++i) {
         double am = 0.0;
+#pragma unroll
         for (int j = 1; j <= 4; ++j) {
             double tmp = fabs(A[I4(i, j)]);
             if (tmp > am) am = tmp;
@@ -81,9 +86,11 @@ VB_HD bool lu_pivot4(double* A, double* t, double* x) {
         if (am == 0.0) return false;
         rn[i - 1] = 1.0 / am;
     }
+#pragma unroll
     for (int k = 1; k <= 4; ++k) {
         int piv = k;
         double pv = fabs(A[I4(k, k)]) * rn[k - 1];
+#pragma unroll
         for (int i = k + 1; i <= 4; ++i) {
             double tmp = fabs(A[I4(i, k)]) * rn[i - 1];
             if (tmp > pv) {
@@ -91,29 +98,38 @@ VB_HD bool lu_pivot4(double* A, double* t, double* x) {
                 piv = i;
             }
         }
-        if (piv != k) {
+#pragma unroll
+        for (int i = k + 1; i <= 4; ++i) {
+            if (piv != i) continue;
+#pragma unroll
             for (int j = 1; j <= 4; ++j) {
                 double tmp = A[I4(k, j)];
-                A[I4(k, j)] = A[I4(piv, j)];
-                A[I4(piv, j)] = tmp;
+                A[I4(k, j)] = A[I4(i, j)];
+                A[I4(i, j)] = tmp;
             }
             double tmp = t[k - 1];
-            t[k - 1] = t[piv - 1];
-            t[piv - 1] = tmp;
+            t[k - 1] = t[i - 1];
+            t[i - 1] = tmp;
             tmp = rn[k - 1];
-            rn[k - 1] = rn[piv - 1];
-            rn[piv - 1] = tmp;
+            rn[k - 1] = rn[i - 1];
+            rn[i - 1] = tmp;
         }
+#pragma unroll
         for (int i = k + 1; i <= 4; ++i) {
             A[I4(i, k)] /= A[I4(k, k)];
+#pragma unroll
             for (int j = k + 1; j <= 4; ++j) A[I4(i, j)] = fma(-A[I4(i, k)], A[I4(k, j)], A[I4(i, j)]);
         }
     }
+#pragma unroll
     for (int i = 1; i <= 4; ++i) {
         x[i - 1] = t[i - 1];
+#pragma unroll
         for (int j = 1; j <= i - 1; ++j) x[i - 1] = fma(-A[I4(i, j)], x[j - 1], x[i - 1]);
     }
+#pragma unroll
     for (int i = 4; i >= 1; --i) {
+#pragma unroll
         for (int j = i + 1; j <= 4; ++j) x[i - 1] = fma(-A[I4(i, j)], x[j - 1], x[i - 1]);
         x[i - 1] /= A[I4(i, i)];
     }

@@ -181,6 +181,17 @@ VB_HD void recon(T q_im2, T q_im1, T q_i, T q_ip1, T q_ip2, T& qr, T& ql) {
         wenoz(q_im2, q_im1, q_i, q_ip1, q_ip2, qr, ql);
 }
 
+// a[i] for a runtime axis i < N, as an unrolled select: the arrays of a face
+// state stay in registers, and no access depends on a runtime index (a
+// runtime-indexed local array read back a stale element in one kernel).
+template <int N, typename T> VB_HD T pick(const T* a, int i) {
+    T r = a[0];
+#pragma unroll
+    for (int k = 1; k < N; ++k)
+        if (k == i) r = a[k];
+    return r;
+}
+
 // ---- EOS and state conversions ---------------------------------------------
 // SoundSpeed, src/eos.jl:15-21
 template <typename T> VB_HD T sound_speed(T rho, T u, T g) {
@@ -209,7 +220,7 @@ template <int DIM, typename T> VB_HD void prim2con(T g, const T* P, T* U) {
 template <int DIM, typename T> VB_HD void prim2flux(int d, T g, const T* P, T* F) {
     T gam = lorentz<DIM>(P);
     T w = g * P[1] + P[0];
-    T un = P[2 + d];
+    T un = pick<DIM>(P + 2, d);
     F[0] = P[0] * un;
     F[1] = -w * un * gam;
 #pragma unroll
@@ -224,7 +235,7 @@ template <int DIM, typename T> VB_HD void prim2flux(int d, T g, const T* P, T* F
 // HARM signal speeds of one state, src/3dim/algos.jl:130-157
 template <int DIM, typename T> VB_HD void harm_speeds(int d, T g, const T* P, T& lp, T& lm) {
     T lor = lorentz<DIM>(P);
-    T v = P[2 + d] / lor;
+    T v = pick<DIM>(P + 2, d) / lor;
     T C = sound_speed(P[0], P[1], g);
     T sig = sq(C) / (sq(lor) * (T(1) - sq(C)));
     T r = sqrt(sig * (T(1) - sq(v) + sig));
@@ -244,7 +255,7 @@ template <int DIM, typename T> struct FaceState {
     VB_HD void make(int d, T g, const T* P) {
         T gam = lorentz<DIM>(P);
         T w = g * P[1] + P[0];
-        T un = P[2 + d];
+        T un = pick<DIM>(P + 2, d);
         U[0] = gam * P[0];
         U[1] = (g - T(1)) * P[1] - sq(gam) * w;
         F[0] = P[0] * un;
@@ -295,48 +306,35 @@ VB_HD void hll_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
 // Verona's conserved vector is (D, -E, m) and its flux (D v_n, -m_n, m v_n + p e_n).
 template <int DIM, typename T>
 VB_HD void hllc_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
+    // Branch-free: the HLL flux and the star-state flux are both formed and
+    // the result is selected once at the end, with the same conditions (and
+    // therefore the same values) as the early-return form of the oracle.
     constexpr int NV = 2 + DIM;
     FaceState<DIM, T> R, L;
     R.make(d, g, PR);
     L.make(d, g, PL);
-    T Cmax = jmax(L.lp, R.lp);
-    T Cmin = -jmin(L.lm, R.lm);
-    if (Cmax < T(0)) {
+    const T Cmax = jmax(L.lp, R.lp);
+    const T Cmin = -jmin(L.lm, R.lm);
+    T Fh[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Fo[v] = R.F[v];
-        return;
-    }
-    if (Cmin < T(0)) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) Fo[v] = L.F[v];
-        return;
-    }
-    T lL = -Cmin, lR = Cmax;
-    T idl = T(1) / (lR - lL);
-    T E_L = -L.U[1], E_R = -R.U[1];
-    T m_L = L.U[2 + d], m_R = R.U[2 + d];
-    T FE_L = -L.F[1], FE_R = -R.F[1];
-    T Fm_L = L.F[2 + d], Fm_R = R.F[2 + d];
-    T E_h = (lR * E_R - lL * E_L - (FE_R - FE_L)) * idl;
-    T m_h = (lR * m_R - lL * m_L - (Fm_R - Fm_L)) * idl;
-    T FE_h = (lR * FE_L - lL * FE_R + lR * lL * (E_R - E_L)) * idl;
-    T Fm_h = (lR * Fm_L - lL * Fm_R + lR * lL * (m_R - m_L)) * idl;
-    T b = E_h + Fm_h;
+    for (int v = 0; v < NV; ++v)
+        Fh[v] = (R.F[v] * Cmin + L.F[v] * Cmax - Cmax * Cmin * (R.U[v] - L.U[v])) / (Cmax + Cmin);
+    const T lL = -Cmin, lR = Cmax;
+    const T idl = T(1) / (lR - lL);
+    const T E_L = -L.U[1], E_R = -R.U[1];
+    const T m_L = pick<DIM>(L.U + 2, d), m_R = pick<DIM>(R.U + 2, d);
+    const T FE_L = -L.F[1], FE_R = -R.F[1];
+    const T Fm_L = pick<DIM>(L.F + 2, d), Fm_R = pick<DIM>(R.F + 2, d);
+    const T E_h = (lR * E_R - lL * E_L - (FE_R - FE_L)) * idl;
+    const T m_h = (lR * m_R - lL * m_L - (Fm_R - Fm_L)) * idl;
+    const T FE_h = (lR * FE_L - lL * FE_R + lR * lL * (E_R - E_L)) * idl;
+    const T Fm_h = (lR * Fm_L - lL * Fm_R + lR * lL * (m_R - m_L)) * idl;
+    const T b = E_h + Fm_h;
     T disc = b * b - T(4) * FE_h * m_h;
     if (disc < T(0)) disc = T(0);
-    T ls = T(2) * m_h / (b + sqrt(disc));
-    T ps = Fm_h - FE_h * ls;
-    // unphysical star state (negative pressure, contact outside the fan, not
-    // finite): fall back to the HLL flux of the same states
-    if (!(ps > T(0)) || !(ls >= lL && ls <= lR)) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v)
-            Fo[v] = (R.F[v] * Cmin + L.F[v] * Cmax - Cmax * Cmin * (R.U[v] - L.U[v])) / (Cmax + Cmin);
-        return;
-    }
-    // star state of the side the contact leaves behind x/t = 0; values are
-    // selected one by one (no pointer to either side's arrays) so that every
-    // array stays in registers
+    const T ls = T(2) * m_h / (b + sqrt(disc));
+    const T ps = Fm_h - FE_h * ls;
+    // star state of the side the contact leaves behind x/t = 0
     const bool left = ls >= T(0);
     T U[NV], F[NV];
 #pragma unroll
@@ -344,20 +342,27 @@ VB_HD void hllc_flux(int d, T g, const T* PL, const T* PR, T* Fo) {
         U[v] = left ? L.U[v] : R.U[v];
         F[v] = left ? L.F[v] : R.F[v];
     }
-    T lK = left ? lL : lR;
-    T vn = left ? L.vn : R.vn;
-    T p = left ? L.p : R.p;
-    T E = -U[1];
-    T fac = (lK - vn) / (lK - ls);
+    const T lK = left ? lL : lR;
+    const T vn = left ? L.vn : R.vn;
+    const T p = left ? L.p : R.p;
+    const T E = -U[1];
+    const T fac = (lK - vn) / (lK - ls);
     T Us[NV];
     Us[0] = U[0] * fac;
 #pragma unroll
-    for (int m = 0; m < DIM; ++m) Us[2 + m] = U[2 + m] * fac;
-    Us[2 + d] = (U[2 + d] * (lK - vn) + ps - p) / (lK - ls);
-    T Es = (E * (lK - vn) + ps * ls - p * vn) / (lK - ls);
+    for (int m = 0; m < DIM; ++m)
+        Us[2 + m] = m == d ? (U[2 + m] * (lK - vn) + ps - p) / (lK - ls) : U[2 + m] * fac;
+    const T Es = (E * (lK - vn) + ps * ls - p * vn) / (lK - ls);
     Us[1] = -Es;
+    // supersonic right / left, unphysical star state -> HLL, else the star flux
+    const bool use_R = Cmax < T(0);
+    const bool use_L = !use_R && Cmin < T(0);
+    const bool use_hll = !use_R && !use_L && (!(ps > T(0)) || !(ls >= lL && ls <= lR));
 #pragma unroll
-    for (int v = 0; v < NV; ++v) Fo[v] = F[v] + lK * (Us[v] - U[v]);
+    for (int v = 0; v < NV; ++v) {
+        const T fs = F[v] + lK * (Us[v] - U[v]);
+        Fo[v] = use_R ? R.F[v] : (use_L ? L.F[v] : (use_hll ? Fh[v] : fs));
+    }
 }
 
 template <int DIM, int RS, typename T>

@@ -87,6 +87,7 @@ __global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
                         DIM > 2 ? NG + (int)blockIdx.z * TZ : 0};
     // valid cells of this (possibly partial) tile along each axis
     int vt[3];
+    #pragma unroll
     for (int a = 0; a < 3; ++a) vt[a] = a < DIM ? min(T[a], p.n[a] - NG - org[a]) : 1;
     const long long vs = p.vs;
     const R fl = R(p.floor_);
@@ -126,11 +127,12 @@ __global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
         const int NF = FX * FY * FZ;
         const int RX = TX + (d == 0 ? 2 : 0), RY = TY + (d == 1 ? 2 : 0), RZ = TZ + (d == 2 ? 2 : 0);
         const int sd = d == 0 ? 1 : (d == 1 ? EX : EX * EY);
-        const int Td = T[d];
+        const int vtd = d == 0 ? vt[0] : (d == 1 ? vt[1] : vt[2]);
         for (int e = tid; e < RX * RY * RZ; e += NT) {
             int rx = e % RX, ry = (e / RX) % RY, rz = e / (RX * RY);
             int c[3] = {rx - (d == 0), ry - (d == 1), rz - (d == 2)};
             bool ok = true;
+            #pragma unroll
             for (int a = 0; a < 3; ++a)
                 ok = ok && (a == d ? (c[a] >= -1 && c[a] <= vt[a]) : c[a] < vt[a]);
             if (!ok) continue;
@@ -138,7 +140,8 @@ __global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
             int base = ex + EX * (ey + EY * ez);
             int fR = c[0] + FX * (c[1] + FY * c[2]);                    // face c_d
             int fL = fR + (d == 0 ? 1 : (d == 1 ? FX : FX * FY));         // face c_d + 1
-            bool wR = c[d] >= 0, wL = c[d] + 1 <= vt[d];
+            const int cd = d == 0 ? c[0] : (d == 1 ? c[1] : c[2]);
+            bool wR = cd >= 0, wL = cd + 1 <= vtd;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 const R* q = sP + v * EXT + base;
@@ -157,6 +160,7 @@ __global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
         for (int e = tid; e < NF; e += NT) {
             int f[3] = {e % FX, (e / FX) % FY, e / (FX * FY)};
             bool ok = true;
+            #pragma unroll
             for (int a = 0; a < 3; ++a) ok = ok && (a == d ? f[a] <= vt[a] : f[a] < vt[a]);
             if (!ok) continue;
             R PL[NV], PR[NV], F[NV];
@@ -183,7 +187,6 @@ __global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
             for (int v = 0; v < NV; ++v)
                 acc[c][v] = acc[c][v] - cdt * ((double)sL[v * NF + flo + fstep] - (double)sL[v * NF + flo]);
         }
-        (void)Td;
     }
 
     // 5. RK combination, con2prim (guess = this stage's input P), Limit
