@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--path", default="both", choices=["both", "fast", "fp64"],
                     help="fp64: time only the plain FP64 path (profiling runs)")
+    ap.add_argument("--guess", default="auto", choices=["auto", "learned", "previous"],
+                    help="con2prim guess of the fast path (auto: learned when the network is available)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
 
@@ -199,7 +201,8 @@ def read_peaks():
 
 
 def read_traffic(key):
-    """Per-cell DRAM bytes of the stage kernel from the committed ncu summary."""
+    """DRAM bytes per cell of one RK-stage kernel group (the stage kernel plus
+    its con2prim kernel where split) from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "stage_kernel_traffic.txt")
     try:
         for line in open(path):
@@ -278,9 +281,18 @@ def run_ours(args, rank, world, dist):
         learned_ok = mlp.available()
     except Exception:
         learned_ok = False
+    if args.guess == "learned" and not learned_ok:
+        raise RuntimeError("--guess learned: the learned con2prim guess is unavailable")
+    if args.guess == "previous":
+        learned_ok = False
     guess = "learned" if learned_ok else "previous"
-    P0 = device_ic(n, 42 + rank)
     info = {}
+    if learned_ok:
+        t0 = time.time()
+        src = "loaded" if os.path.exists(mlp.DEFAULT_WEIGHTS) else "trained"
+        mlp.trained()
+        info["mlp"] = {"weights": src, "seconds": round(time.time() - t0, 2), "params": mlp.n_params()}
+    P0 = device_ic(n, 42 + rank)
 
     # plain FP64 path (same scheme, reference con2prim)
     fp64 = None
@@ -350,13 +362,17 @@ def run_ours(args, rank, world, dist):
 
     if rank != 0:
         return
-    # roofline of the dominant kernel (the fused stage kernel): algorithmic bytes
-    # per zone-update for FP32-bulk SSP-RK3 = 6*5*4 (P) + 8*5*8 (U) = 440 B
+    # roofline of the dominant kernel group (one RK stage: the z-marching stage
+    # kernel and its con2prim kernel). Algorithmic bytes per zone-update of an
+    # FP32-bulk SSP-RK3 step: P read and written once per stage, 3 * 2 * 5 * 4 B
+    # = 120 B, and the FP64 conserved arrays, 8 passes of 5 * 8 B (stage 1: U^n
+    # in, U^1 out; stages 2, 3: U^n and U^(k-1) in, U^k out) = 320 B; 440 B in
+    # all, 440/3 B per cell per stage launch.
     peak, peak_kind = read_peaks()
     bytes_per_cell_step = 440.0
-    stage_ms_per_step = st_ms / K
-    achieved = cells * bytes_per_cell_step / (stage_ms_per_step / 1e3) / 1e9
-    traffic = read_traffic("fp32_wenoz_hllc_rk3")
+    stage_ms_per_launch = st_ms / max(st_l, 1)
+    achieved = cells * bytes_per_cell_step / 3.0 / (stage_ms_per_launch / 1e3) / 1e9
+    traffic = read_traffic(f"fp32_{guess}_stage_group")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -366,10 +382,11 @@ def run_ours(args, rank, world, dist):
         "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
         "l1_error_vs_fp64": err,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic * cells / 3 if traffic else None, "peak_kind": peak_kind,
-                     "kernel": "k_stage (fused reconstruct+HLLC+divergence+RK+con2prim)",
-                     "algorithmic_bytes_per_zone_update": bytes_per_cell_step,
-                     "stage_ms_per_launch": st_ms / max(st_l, 1)},
+                     "traffic": traffic * cells if traffic else None, "peak_kind": peak_kind,
+                     "per": "one RK-stage launch of the kernel group over the full grid",
+                     "kernel": "k_stage_zm (reconstruct+HLLC+divergence+RK) + con2prim kernel",
+                     "algorithmic_bytes_per_launch": bytes_per_cell_step / 3.0 * cells,
+                     "stage_ms_per_launch": stage_ms_per_launch},
         "gpu_launches": launches,
         "clocks": clk.summary,
         "e2e": e2e,

@@ -192,7 +192,7 @@ int vb_point_con2prim(int dims, double gamma, int n_iter, double tol, const doub
 
 /* ---- learned con2prim guess (extension; the reference warm-starts Newton from
  * the previous primitive state, src/3dim/structs.jl:277-287) ----------------------
- * A 4 -> 64 -> 64 -> 64 -> 1 SiLU MLP in BF16 on the tensor cores (tcgen05, FP32
+ * A 4 -> 64 -> 64 -> 64 -> 1 ReLU MLP in BF16 on the tensor cores (tcgen05, FP32
  * accumulation in TMEM). With E = tau + D = -U2: features f = (log D, |S|/E,
  * log(E/D), Gamma) normalised by norm = {mean[4], 1/std[4]}; output y, the
  * pressure guess as a fraction of E: p0 = E max(y, 0), Newton start

@@ -1,6 +1,6 @@
 """CPU reference of the learned con2prim guess network -- TEST INFRASTRUCTURE ONLY.
 
-Forward and backward of the 4 -> 64 -> 64 -> 64 -> 1 SiLU MLP in FP64 numpy,
+Forward and backward of the 4 -> 64 -> 64 -> 64 -> 1 ReLU MLP in FP64 numpy,
 with the parameter layout of include/verona_b200.h (W[in][out]). `bf16=True`
 rounds the tensor-core operands (features, h1, h2, weights) to bfloat16 as the
 GPU does, so the forward can be compared tightly; gradients are compared
@@ -37,24 +37,23 @@ def bf16(x):
     return u.view(np.float32).astype(np.float64)
 
 
-def silu(z):
-    return z / (1.0 + np.exp(-z))
+def relu(z):
+    return np.maximum(z, 0.0)
 
 
-def dsilu(z):
-    s = 1.0 / (1.0 + np.exp(-z))
-    return s * (1.0 + z * (1.0 - s))
+def drelu(z):
+    return (z > 0.0).astype(np.float64)
 
 
 def forward(params, x, bf=False):
     p = split(params)
     q = (lambda a: bf16(a)) if bf else (lambda a: a)
     z1 = q(x) @ q(p["W1"])
-    h1 = silu(z1 + p["b1"])
+    h1 = relu(z1 + p["b1"])
     z2 = q(h1) @ q(p["W2"])
-    h2 = silu(z2 + p["b2"])
+    h2 = relu(z2 + p["b2"])
     z3 = q(h2) @ q(p["W3"])
-    h3 = silu(z3 + p["b3"])
+    h3 = relu(z3 + p["b3"])
     y = h3 @ p["w4"] + p["b4"][0]
     return y, (z1, h1, z2, h2, z3, h3)
 
@@ -67,13 +66,13 @@ def loss_and_grad(params, x, t):
     r = y - t
     dy = 2.0 * r / n
     g = {"w4": h3.T @ dy, "b4": np.array([dy.sum()])}
-    dz3 = np.outer(dy, p["w4"]) * dsilu(z3 + p["b3"])
+    dz3 = np.outer(dy, p["w4"]) * drelu(z3 + p["b3"])
     g["W3"] = h2.T @ dz3
     g["b3"] = dz3.sum(0)
-    dz2 = (dz3 @ p["W3"].T) * dsilu(z2 + p["b2"])
+    dz2 = (dz3 @ p["W3"].T) * drelu(z2 + p["b2"])
     g["W2"] = h1.T @ dz2
     g["b2"] = dz2.sum(0)
-    dz1 = (dz2 @ p["W2"].T) * dsilu(z1 + p["b1"])
+    dz1 = (dz2 @ p["W2"].T) * drelu(z1 + p["b1"])
     g["W1"] = x.T @ dz1
     g["b1"] = dz1.sum(0)
     return float(np.mean(r * r)), join(g)

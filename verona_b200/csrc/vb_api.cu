@@ -57,6 +57,7 @@ struct vb_solver {
     // learned con2prim guess
     const void* mlp_blob = nullptr;
     unsigned int* tc_err = nullptr;
+    float* w_guess = nullptr;  // one W guess per padded cell
     // profiling
     bool prof = false;
     std::vector<cudaEvent_t> ev;
@@ -144,6 +145,7 @@ int vb_destroy(vb_handle h) {
     cudaFree(h->partial);
     cudaFree(h->staging);
     cudaFree(h->tc_err);
+    cudaFree(h->w_guess);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     cudaSetDevice(prev);
     delete h;
@@ -427,14 +429,21 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
             if (rc2) return rc2;
             VB_CUDA(h, cudaEventRecord(e0, s));
         }
-        VB_CUDA(h, launch_stage<R>(h->dims, h->opt.recon, h->opt.riemann, p, bufs, s));
+        int nk = 0;
+        VB_CUDA(h, launch_stage<R>(h->dims, h->opt.recon, h->opt.riemann, p, bufs, s, &nk));
         if (p.skip_c2p) {
-            VB_CUDA(h, launch_c2p_learned(h->mlp_blob, p, Pin, Pout, fp32(h), Uo, h->tc_err, s));
-            h->launches += 1;
+            // learned guess: the network's W per cell, then the W Newton from it
+            VB_CUDA(h, launch_mlp_guess(h->mlp_blob, p, Uo, h->w_guess, h->tc_err, s));
+            StageParams q = p;
+            q.skip_c2p = 0;
+            q.c2p_mode = C2P_GUESS_W;
+            q.w_guess = h->w_guess;
+            VB_CUDA(h, launch_c2p<R>(q, bufs, s));
+            h->launches += 2;
         }
         if (h->prof) VB_CUDA(h, cudaEventRecord(e1, s));
         VB_CUDA(h, launch_ghost_limit<R>(g, Pin, Pout, h->opt.floor_, s));
-        h->launches += 2 + (p.split && h->dims == 3 ? 1 : 0);
+        h->launches += nk + 1;
         h->stage_launches += 1;
         return VB_OK;
     };
@@ -551,6 +560,10 @@ int vb_profile_read(vb_handle h, double* stage_ms, int64_t* stage_launches, int6
 int vb_attach_mlp(vb_handle h, vb_mlp_handle m) {
     if (!h || !m) return fail(h, VB_ERR_ARG, "vb_attach_mlp: null argument");
     if (h->dims != 3 || h->nghost != 3) return fail(h, VB_ERR_UNSUPPORTED, "vb_attach_mlp: 3D grids only");
+    if (!h->w_guess) {
+        int rc = dev_alloc(h, (void**)&h->w_guess, sizeof(float) * (size_t)h->vs);
+        if (rc) return rc;
+    }
     if (!h->tc_err) {
         int rc = dev_alloc(h, (void**)&h->tc_err, sizeof(unsigned int));
         if (rc) return rc;

@@ -58,7 +58,7 @@ struct Grid {
 // R = float (vb_stage_f32.cu) --------------------------------------------------
 template <typename R>
 cudaError_t launch_stage(int dims, int rec, int rs, const StageParams& p, const StageBufs<R>& b,
-                         cudaStream_t s);
+                         cudaStream_t s, int* kernels);
 // AoS (Julia column-major, variable fastest) FP64 -> internal SoA R; also U0 = PtoU(P) in FP64
 template <typename R>
 cudaError_t launch_load_prims(const Grid& g, const double* P_aos, R* P, double* U0, double gamma,
@@ -90,9 +90,13 @@ cudaError_t launch_ref1d_store(const Ref1DState& st, double* P_aos, cudaStream_t
 
 int max_speed_blocks(const Grid& g);
 
-// learned-guess con2prim of a split stage (vb_mlp.cu)
-cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const void* Pin, void* Pout, bool fp32,
-                               const double* Uo, unsigned int* err, cudaStream_t s);
+// split con2prim of a 3D stage on its own (vb_stage_zm.cuh)
+template <typename R> cudaError_t launch_c2p(const StageParams& p, const StageBufs<R>& b, cudaStream_t s);
+
+// learned guess of a split stage (vb_mlp.cu): W guess per interior cell of U
+// (padded SoA, the grid of p) into w_guess (one float per padded cell)
+cudaError_t launch_mlp_guess(const void* mlp_blob, const StageParams& p, const double* U, float* w_guess,
+                             unsigned int* err, cudaStream_t s);
 
 // point kernels (FP64, vb_stage_f64.cu)
 cudaError_t launch_point_recon(int method, const double* q, double* out, int n, cudaStream_t s);

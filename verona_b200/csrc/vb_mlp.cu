@@ -1,4 +1,4 @@
-// Learned con2prim initial guess: a 4 -> 64 -> 64 -> 64 -> 1 SiLU MLP in
+// Learned con2prim initial guess: a 4 -> 64 -> 64 -> 64 -> 1 ReLU MLP in
 // BF16 on the sm_100a tensor cores (tcgen05, FP32 accumulation in TMEM).
 //
 // Inputs per cell (the conserved state only), with E = tau + D = -U2 the
@@ -17,7 +17,14 @@
 //                   tensor-core layout (forward W^T and backward W copies)
 //   k_mlp_features  conserved states -> normalised features and targets
 //   k_mlp_forward   features -> y, 128 cells per tile (inference only)
-//   k_c2p_learned   split-stage con2prim: U -> features -> MLP -> W0 -> Newton
+//   k_mlp_guess     split-stage guess: U -> features -> MLP -> W0 per cell;
+//                   the stage's con2prim kernel then runs the W Newton from it
+//
+// Inference folds every bias into its MMA: the activation operand carries two
+// constant columns of ones and the weight operand the bias split into a BF16
+// high part and a BF16 remainder (bias error ~2^-17 relative), so an epilogue
+// is one TMEM load, ReLU + BF16 packing in one cvt per pair, and the shared
+// stores of the next operand.
 //   k_mlp_train     forward + backward of 128-sample tiles; every GEMM
 //                   (three forward layers, two backward input-gradients and
 //                   all weight/bias gradients) runs as tcgen05.mma; weight
@@ -42,6 +49,7 @@
 namespace vb {
 
 constexpr int MLP_IN = 4, MLP_H = 64, MLP_KIN = 16;  // layer-1 K padded to one MMA
+constexpr int MLP_KH = MLP_H + 16;                   // inference K of layers 2, 3: 64 + bias columns
 constexpr int TILE = 128;                            // cells per tile = MMA M
 constexpr uint32_t MAX_POLLS = 1u << 26;             // bounded mbarrier waits
 // FP32 master parameter vector: W1[4][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] w4[64] b4
@@ -56,6 +64,9 @@ struct MlpBlob {
     __nv_bfloat16 w3t[MLP_H * MLP_H];    // B of layer 3
     __nv_bfloat16 w2n[MLP_H * MLP_H];    // B of dh1 = dz2 W2^T: rows = in, K = out
     __nv_bfloat16 w3n[MLP_H * MLP_H];    // B of dh2 = dz3 W3^T
+    __nv_bfloat16 w1i[MLP_H * MLP_KIN];  // inference B of layer 1: W1^T, b1 high, b1 remainder in K 4, 5
+    __nv_bfloat16 w2i[MLP_H * MLP_KH];   // inference B of layer 2: W2^T, b2 high, b2 remainder in K 64, 65
+    __nv_bfloat16 w3i[MLP_H * MLP_KH];   // inference B of layer 3
     float b1[MLP_H], b2[MLP_H], b3[MLP_H], w4[MLP_H];
     float b4;
     float mu[MLP_IN], isd[MLP_IN];
@@ -68,11 +79,8 @@ __device__ __forceinline__ bool cta_wait(uint64_t* mbar, uint32_t parity, unsign
     return !__syncthreads_or(!ok);
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
-__device__ __forceinline__ float dsilu(float z) {
-    float s = 1.0f / (1.0f + __expf(-z));
-    return s * (1.0f + z * (1.0f - s));
-}
+__device__ __forceinline__ float relu(float z) { return fmaxf(z, 0.0f); }
+__device__ __forceinline__ float drelu(float z) { return z > 0.0f ? 1.0f : 0.0f; }
 
 // ---- features -------------------------------------------------------------------
 __device__ __forceinline__ void cell_features(const double* U, double gamma, const float* mu, const float* isd,
@@ -108,6 +116,25 @@ __global__ void k_mlp_pack(const float* __restrict__ prm, const float* __restric
             __float2bfloat16(w2);
         *reinterpret_cast<__nv_bfloat16*>(base + offsetof(MlpBlob, w3n) + tc::kmajor_off(MLP_H, a, c)) =
             __float2bfloat16(w3);
+    }
+    // inference operands with the biases as two extra K columns (high + remainder)
+    auto put = [&](size_t off, int R, int row, int k, float v) {
+        *reinterpret_cast<__nv_bfloat16*>(base + off + tc::kmajor_off(R, row, k)) = __float2bfloat16(v);
+    };
+    auto hi = [](float b) { return __bfloat162float(__float2bfloat16(b)); };
+    for (int e = t; e < MLP_H * MLP_KIN; e += stride) {
+        int o = e / MLP_KIN, i = e % MLP_KIN;
+        float b = prm[OFF_B1 + o];
+        float w = i < MLP_IN ? prm[OFF_W1 + i * MLP_H + o] : (i == MLP_IN ? hi(b) : (i == MLP_IN + 1 ? b - hi(b) : 0.0f));
+        put(offsetof(MlpBlob, w1i), MLP_H, o, i, w);
+    }
+    for (int e = t; e < MLP_H * MLP_KH; e += stride) {
+        int o = e / MLP_KH, a = e % MLP_KH;  // row = out o, K = in a
+        float b2 = prm[OFF_B2 + o], b3 = prm[OFF_B3 + o];
+        float w2 = a < MLP_H ? prm[OFF_W2 + a * MLP_H + o] : (a == MLP_H ? hi(b2) : (a == MLP_H + 1 ? b2 - hi(b2) : 0.0f));
+        float w3 = a < MLP_H ? prm[OFF_W3 + a * MLP_H + o] : (a == MLP_H ? hi(b3) : (a == MLP_H + 1 ? b3 - hi(b3) : 0.0f));
+        put(offsetof(MlpBlob, w2i), MLP_H, o, a, w2);
+        put(offsetof(MlpBlob, w3i), MLP_H, o, a, w3);
     }
     for (int e = t; e < MLP_H; e += stride) {
         blob->b1[e] = prm[OFF_B1 + e];
@@ -148,40 +175,52 @@ __global__ void k_mlp_features(const double* __restrict__ U, const double* __res
 
 // ---- shared memory of the inference path -------------------------------------------------
 struct InferSmem {
-    __nv_bfloat16 a1[TILE * MLP_KIN];  // layer-1 input, K-major
-    __nv_bfloat16 h[TILE * MLP_H];     // h1, then h2
-    __nv_bfloat16 w1t[MLP_H * MLP_KIN];
-    __nv_bfloat16 w2t[MLP_H * MLP_H];
-    __nv_bfloat16 w3t[MLP_H * MLP_H];
-    float b1[MLP_H], b2[MLP_H], b3[MLP_H], w4[MLP_H];
+    __nv_bfloat16 a1[TILE * MLP_KIN];  // layer-1 input [cells x 16]: 4 features, 1, 1, zeros
+    __nv_bfloat16 h[TILE * MLP_KH];    // h1, then h2 [cells x 80]: 64 activations, 1, 1, zeros
+    __nv_bfloat16 w1i[MLP_H * MLP_KIN];
+    __nv_bfloat16 w2i[MLP_H * MLP_KH];
+    __nv_bfloat16 w3i[MLP_H * MLP_KH];
+    float w4[MLP_H];
     float b4, mu[MLP_IN], isd[MLP_IN];
     uint64_t mbar;
     uint32_t tmem_base;
 };
 
+__device__ __forceinline__ uint32_t bf16x2(float lo, float hi) {
+    __nv_bfloat162 p = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&p);
+}
+// max(lo, 0), max(hi, 0) rounded to BF16 and packed (lo in the low half)
+__device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
+// Weights into shared memory, and the constant columns of the activation
+// operand h (K 64, 65 = 1 multiply the bias columns of w2i / w3i; 66..79 = 0).
 __device__ void load_weights_infer(InferSmem& s, const MlpBlob* __restrict__ blob) {
     const int t = threadIdx.x, nt = blockDim.x;
-    const uint4* src1 = reinterpret_cast<const uint4*>(blob->w1t);
-    uint4* dst1 = reinterpret_cast<uint4*>(s.w1t);
-    for (int i = t; i < (int)(sizeof(s.w1t) / 16); i += nt) dst1[i] = src1[i];
-    const uint4* src2 = reinterpret_cast<const uint4*>(blob->w2t);
-    uint4* dst2 = reinterpret_cast<uint4*>(s.w2t);
-    for (int i = t; i < (int)(sizeof(s.w2t) / 16); i += nt) dst2[i] = src2[i];
-    const uint4* src3 = reinterpret_cast<const uint4*>(blob->w3t);
-    uint4* dst3 = reinterpret_cast<uint4*>(s.w3t);
-    for (int i = t; i < (int)(sizeof(s.w3t) / 16); i += nt) dst3[i] = src3[i];
-    for (int i = t; i < MLP_H; i += nt) {
-        s.b1[i] = blob->b1[i];
-        s.b2[i] = blob->b2[i];
-        s.b3[i] = blob->b3[i];
-        s.w4[i] = blob->w4[i];
-    }
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+        const uint4* x = reinterpret_cast<const uint4*>(src);
+        uint4* y = reinterpret_cast<uint4*>(dst);
+        for (int i = t; i < (int)(bytes / 16); i += nt) y[i] = x[i];
+    };
+    cp(s.w1i, blob->w1i, sizeof(s.w1i));
+    cp(s.w2i, blob->w2i, sizeof(s.w2i));
+    cp(s.w3i, blob->w3i, sizeof(s.w3i));
+    for (int i = t; i < MLP_H; i += nt) s.w4[i] = blob->w4[i];
     if (t == 0) {
         s.b4 = blob->b4;
         for (int i = 0; i < MLP_IN; ++i) {
             s.mu[i] = blob->mu[i];
             s.isd[i] = blob->isd[i];
         }
+    }
+    char* hb = reinterpret_cast<char*>(s.h);
+    for (int r = t; r < TILE; r += nt) {
+        *reinterpret_cast<uint4*>(hb + tc::kmajor_off(TILE, r, MLP_H)) = make_uint4(bf16x2(1.0f, 1.0f), 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(hb + tc::kmajor_off(TILE, r, MLP_H + 8)) = make_uint4(0u, 0u, 0u, 0u);
     }
 }
 
@@ -216,43 +255,61 @@ __device__ __forceinline__ void store_row16(__nv_bfloat16* buf, int row, const f
     *reinterpret_cast<uint4*>(b + tc::kmajor_off(TILE, row, 8)) = make_uint4(0u, 0u, 0u, 0u);
 }
 
-// One MLP forward for the CTA's 128 cells (thread t = cell/row t). f: this
-// thread's 4 normalised features; returns y = log(p/D). The caller holds TMEM
-// (64 columns at s.tmem_base) and the mbarrier; `phase` counts completed
-// commits. Returns false if a bounded wait ran out.
+// ReLU of 64 FP32 accumulators, as BF16, into row `row` (K 0..63) of the
+// K-major [TILE x 80] activation operand
+__device__ __forceinline__ void store_row64_relu(__nv_bfloat16* buf, int row, const float* v) {
+    char* b = reinterpret_cast<char*>(buf);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        uint4 q;
+        q.x = relu_bf16x2(v[8 * c + 0], v[8 * c + 1]);
+        q.y = relu_bf16x2(v[8 * c + 2], v[8 * c + 3]);
+        q.z = relu_bf16x2(v[8 * c + 4], v[8 * c + 5]);
+        q.w = relu_bf16x2(v[8 * c + 6], v[8 * c + 7]);
+        *reinterpret_cast<uint4*>(b + tc::kmajor_off(TILE, row, 8 * c)) = q;
+    }
+}
+
+// One MLP forward for the CTA's 128 cells (thread t = cell / row t). f: this
+// thread's 4 normalised features; returns y, the predicted p / E. The caller
+// holds TMEM (64 columns at s.tmem_base) and the mbarrier; `phase` counts
+// completed commits. Returns false if a bounded wait ran out.
 __device__ bool mlp_forward_tile(InferSmem& s, const float* f, float& y, uint32_t& phase, unsigned int* err) {
     const int t = threadIdx.x, warp = t >> 5;
     const uint32_t tmem = s.tmem_base;
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
     constexpr uint32_t ID64 = tc::idesc_bf16_f32(TILE, MLP_H);
-    store_row16(s.a1, t, f);
+    {
+        char* b = reinterpret_cast<char*>(s.a1);
+        *reinterpret_cast<uint4*>(b + tc::kmajor_off(TILE, t, 0)) =
+            make_uint4(bf16x2(f[0], f[1]), bf16x2(f[2], f[3]), bf16x2(1.0f, 1.0f), 0u);
+        *reinterpret_cast<uint4*>(b + tc::kmajor_off(TILE, t, 8)) = make_uint4(0u, 0u, 0u, 0u);
+    }
     tc::fence_proxy_async();
     __syncthreads();
     float z[64];
-    // layer 1 (K = 16: one MMA)
+    // layer 1 (K = 16: one MMA; bias in K 4, 5)
     if (t == 0) {
         tc::fence_after_sync();
-        tc::mma_bf16(tmem, tc::operand_desc(s.a1, TILE, 0), tc::operand_desc(s.w1t, MLP_H, 0), ID64, 0);
+        tc::mma_bf16(tmem, tc::operand_desc(s.a1, TILE, 0), tc::operand_desc(s.w1i, MLP_H, 0), ID64, 0);
         tc::mma_commit(&s.mbar);
     }
     if (!cta_wait(&s.mbar, phase & 1, err)) return false;
     ++phase;
     tc::fence_after_sync();
     tc::tmem_ld64(trow, z);
-#pragma unroll
-    for (int i = 0; i < 64; ++i) z[i] = silu(z[i] + s.b1[i]);
-    store_row64(s.h, t, z);
+    store_row64_relu(s.h, t, z);
     tc::fence_proxy_async();
     tc::fence_before_sync();
     __syncthreads();
-    // layers 2 and 3 (K = 64: four MMAs each)
+    // layers 2 and 3 (K = 80: five MMAs each; bias in K 64, 65)
+#pragma unroll 1
     for (int layer = 0; layer < 2; ++layer) {
-        const __nv_bfloat16* w = layer == 0 ? s.w2t : s.w3t;
-        const float* bias = layer == 0 ? s.b2 : s.b3;
+        const __nv_bfloat16* w = layer == 0 ? s.w2i : s.w3i;
         if (t == 0) {
             tc::fence_after_sync();
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
+            for (int k = 0; k < MLP_KH / 16; ++k)
                 tc::mma_bf16(tmem, tc::operand_desc(s.h, TILE, k), tc::operand_desc(w, MLP_H, k), ID64, k > 0);
             tc::mma_commit(&s.mbar);
         }
@@ -260,10 +317,8 @@ __device__ bool mlp_forward_tile(InferSmem& s, const float* f, float& y, uint32_
         ++phase;
         tc::fence_after_sync();
         tc::tmem_ld64(trow, z);
-#pragma unroll
-        for (int i = 0; i < 64; ++i) z[i] = silu(z[i] + bias[i]);
         if (layer == 0) {  // the layer-2 MMA has completed: h1 can be overwritten by h2
-            store_row64(s.h, t, z);
+            store_row64_relu(s.h, t, z);
             tc::fence_proxy_async();
             tc::fence_before_sync();
             __syncthreads();
@@ -271,11 +326,32 @@ __device__ bool mlp_forward_tile(InferSmem& s, const float* f, float& y, uint32_
     }
     float acc = s.b4;
 #pragma unroll
-    for (int i = 0; i < 64; ++i) acc = fmaf(s.w4[i], z[i], acc);
+    for (int i = 0; i < 64; ++i) acc = fmaf(s.w4[i], relu(z[i]), acc);
     y = acc;
     tc::fence_before_sync();
     __syncthreads();  // all TMEM loads of this tile done before the next tile's MMA
     return true;
+}
+
+// shared prologue / epilogue of the inference kernels: weights, TMEM, mbarrier.
+// The allocation permit is given up right after the allocation: a CTA that
+// still holds it keeps the next CTA of the kernel off the SM.
+__device__ __forceinline__ void infer_begin(InferSmem& s, const MlpBlob* __restrict__ blob) {
+    load_weights_infer(s, blob);
+    if (threadIdx.x < 32) {
+        tc::tmem_alloc(&s.tmem_base, 64);
+        tc::tmem_relinquish();
+    }
+    if (threadIdx.x == 0) tc::mbar_init(&s.mbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+}
+__device__ __forceinline__ void infer_end(InferSmem& s) {
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x < 32) tc::tmem_dealloc(s.tmem_base, 64);
 }
 
 __global__ void __launch_bounds__(TILE) k_mlp_forward(const MlpBlob* __restrict__ blob, const float* __restrict__ feat,
@@ -283,13 +359,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const MlpBlob* __restrict_
     extern __shared__ __align__(128) unsigned char smraw[];
     InferSmem& s = *reinterpret_cast<InferSmem*>(smraw);
     const int t = threadIdx.x;
-    load_weights_infer(s, blob);
-    if (t < 32) tc::tmem_alloc(&s.tmem_base, 64);
-    if (t == 0) tc::mbar_init(&s.mbar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
+    infer_begin(s, blob);
     uint32_t phase = 0;
     const int ntiles = (n + TILE - 1) / TILE;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -301,101 +371,77 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const MlpBlob* __restrict_
         if (!mlp_forward_tile(s, f, y, phase, err)) break;
         if (i < n) out[i] = y;
     }
-    __syncthreads();
-    if (t < 32) {
-        tc::tmem_relinquish();
-        tc::tmem_dealloc(s.tmem_base, 64);
-    }
+    infer_end(s);
 }
 
-// ---- split-stage con2prim with the learned guess -----------------------------------------
-struct LearnedC2PArgs {
+// ---- learned W guesses of a split stage ------------------------------------------------
+struct GuessArgs {
     int n[3];
     long long sy, sz, vs;
-    double gamma, floor_, rtol;
-    int max_newton, max_bracket, stats;
-    const float* Pin_f;  // FP32-bulk primitive input (or null)
-    const double* Pin_d; // FP64 primitive input (or null)
-    float* Pout_f;
-    double* Pout_d;
-    const double* Uo;
-    unsigned long long* counters;
+    float gamma;
+    const double* U;  // conserved state of the stage, padded SoA
+    float* w_guess;   // one per padded cell (interior cells written)
     unsigned int* err;
 };
 
-__global__ void __launch_bounds__(TILE) k_c2p_learned(const MlpBlob* __restrict__ blob, LearnedC2PArgs a) {
+// the features of cell_features in FP32 arithmetic (they feed a BF16 network)
+__device__ __forceinline__ void guess_features(const double* U, float gamma, const float* mu, const float* isd,
+                                               float* f) {
+    const float D = (float)U[0], E = (float)(-U[1]);
+    const float S = sqrtf((float)(U[2] * U[2] + U[3] * U[3] + U[4] * U[4]));
+    const float raw[4] = {__logf(fmaxf(D, 1e-30f)), __fdividef(S, E), __logf(fmaxf(__fdividef(E, D), 1e-30f)), gamma};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) f[i] = (raw[i] - mu[i]) * isd[i];
+}
+
+// interior cell e of the grid -> padded linear index; false past the end
+__device__ __forceinline__ bool guess_cell(const GuessArgs& a, long long e, long long tot, int N0, int N1,
+                                           long long& c) {
+    if (e >= tot) return false;
+    const int i = (int)(e % N0) + NG;
+    const int j = (int)((e / N0) % N1) + NG;
+    const int k = (int)(e / ((long long)N0 * N1)) + NG;
+    c = i + a.sy * j + a.sz * k;
+    return true;
+}
+
+// One thread per cell of a 128-cell tile; the next tile's state is loaded
+// before the current tile's network runs.
+__global__ void __launch_bounds__(TILE) k_mlp_guess(const MlpBlob* __restrict__ blob, GuessArgs a) {
     extern __shared__ __align__(128) unsigned char smraw[];
     InferSmem& s = *reinterpret_cast<InferSmem*>(smraw);
     const int t = threadIdx.x;
-    load_weights_infer(s, blob);
-    if (t < 32) tc::tmem_alloc(&s.tmem_base, 64);
-    if (t == 0) tc::mbar_init(&s.mbar, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
+    infer_begin(s, blob);
     const int N0 = a.n[0] - 2 * NG, N1 = a.n[1] - 2 * NG, N2 = a.n[2] - 2 * NG;
     const long long tot = (long long)N0 * N1 * N2;
     const long long ntiles = (tot + TILE - 1) / TILE;
     uint32_t phase = 0;
-    unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long e = tile * TILE + t;
-        const bool ok = e < tot;
-        long long c = 0;
-        double U[5] = {1.0, -2.0, 0.0, 0.0, 0.0};
-        if (ok) {
-            const int i = (int)(e % N0) + NG;
-            const int j = (int)((e / N0) % N1) + NG;
-            const int k = (int)(e / ((long long)N0 * N1)) + NG;
-            c = i + a.sy * j + a.sz * k;
+    long long tile = blockIdx.x;
+    long long c = 0;
+    bool ok = tile < ntiles && guess_cell(a, tile * TILE + t, tot, N0, N1, c);
+    double u[5] = {1.0, -2.0, 0.0, 0.0, 0.0};
+    if (ok)
 #pragma unroll
-            for (int v = 0; v < 5; ++v) U[v] = a.Uo[v * a.vs + c];
-        }
+        for (int v = 0; v < 5; ++v) u[v] = a.U[v * a.vs + c];
+    for (; tile < ntiles; tile += gridDim.x) {
+        const long long nt = tile + gridDim.x;
+        long long cn = 0;
+        const bool okn = nt < ntiles && guess_cell(a, nt * TILE + t, tot, N0, N1, cn);
+        double un[5] = {1.0, -2.0, 0.0, 0.0, 0.0};
+        if (okn)
+#pragma unroll
+            for (int v = 0; v < 5; ++v) un[v] = a.U[v * a.vs + cn];
         float f[4];
-        double ld;
-        cell_features(U, a.gamma, s.mu, s.isd, f, &ld);
+        guess_features(u, a.gamma, s.mu, s.isd, f);
         float y = 0.f;
         if (!mlp_forward_tile(s, f, y, phase, a.err)) break;
-        if (!ok) continue;
-        const double W0 = -U[1] * (1.0 + fmax((double)y, 0.0));
-        double P[5];
-        int fb;
-        int r = c2p_w(a.gamma, U, W0, a.rtol, a.max_newton, a.max_bracket, P, &fb);
-        n_fail += (r < 0);
-        n_fb += fb;
-        n_it += (r < 0 ? -r : r);
-        n_cells += 1;
-        P[0] = jmax(P[0], a.floor_);
-        P[1] = jmax(P[1], a.floor_);
+        if (ok) a.w_guess[c] = (float)(-u[1] * (1.0 + (double)fmaxf(y, 0.0f)));
+        ok = okn;
+        c = cn;
 #pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            if (a.Pout_f)
-                a.Pout_f[v * a.vs + c] = (float)P[v];
-            else
-                a.Pout_d[v * a.vs + c] = P[v];
-        }
+        for (int v = 0; v < 5; ++v) u[v] = un[v];
     }
-    __syncthreads();
-    if (t < 32) {
-        tc::tmem_relinquish();
-        tc::tmem_dealloc(s.tmem_base, 64);
-    }
-    if (n_fail) atomicAdd(a.counters + CNT_C2P_FAIL, n_fail);
-    if (a.stats) {
-        for (int o = 16; o > 0; o >>= 1) {
-            n_fb += __shfl_xor_sync(0xffffffffu, n_fb, o);
-            n_it += __shfl_xor_sync(0xffffffffu, n_it, o);
-            n_cells += __shfl_xor_sync(0xffffffffu, n_cells, o);
-        }
-        if ((t & 31) == 0) {
-            if (n_fb) atomicAdd(a.counters + CNT_C2P_FALLBACK, n_fb);
-            if (n_it) atomicAdd(a.counters + CNT_C2P_ITERS, n_it);
-            if (n_cells) atomicAdd(a.counters + CNT_C2P_CELLS, n_cells);
-        }
-    } else if (n_fb) {
-        atomicAdd(a.counters + CNT_C2P_FALLBACK, n_fb);
-    }
+    infer_end(s);
 }
 
 // ---- training ---------------------------------------------------------------------
@@ -474,7 +520,10 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict
         for (int i = t; i < (int)(sizeof(s.at) / 16); i += TILE) reinterpret_cast<uint4*>(s.at)[i] = z;
         for (int i = t; i < (int)(sizeof(s.dyt) / 16); i += TILE) reinterpret_cast<uint4*>(s.dyt)[i] = z;
     }
-    if (t < 32) tc::tmem_alloc(&s.tmem_base, TC_NCOL);
+    if (t < 32) {
+        tc::tmem_alloc(&s.tmem_base, TC_NCOL);
+        tc::tmem_relinquish();  // a CTA holding the permit keeps the next CTA off the SM
+    }
     if (t == 0) tc::mbar_init(&s.mbar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     tc::fence_before_sync();
@@ -507,7 +556,7 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict
         if (!good) break;
         tc::tmem_ld64(tm + lanebase + TC_Z1, z);
 #pragma unroll
-        for (int k = 0; k < 64; ++k) g[k] = silu(z[k] + s.b1[k]);
+        for (int k = 0; k < 64; ++k) g[k] = relu(z[k] + s.b1[k]);
         store_row64(s.h, t, g);
         good = run_mma(s, phase, err, [&] {
 #pragma unroll
@@ -517,7 +566,7 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict
         if (!good) break;
         tc::tmem_ld64(tm + lanebase + TC_Z2, z);
 #pragma unroll
-        for (int k = 0; k < 64; ++k) g[k] = silu(z[k] + s.b2[k]);
+        for (int k = 0; k < 64; ++k) g[k] = relu(z[k] + s.b2[k]);
         store_row64(s.h, t, g);
         good = run_mma(s, phase, err, [&] {
 #pragma unroll
@@ -529,7 +578,7 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict
         float y = s.b4;
 #pragma unroll
         for (int k = 0; k < 64; ++k) {
-            g[k] = silu(z[k] + s.b3[k]);
+            g[k] = relu(z[k] + s.b3[k]);
             y = fmaf(s.w4[k], g[k], y);
         }
         const float r = ok ? (y - tgt) : 0.0f;
@@ -540,9 +589,9 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict
         for (int k = 0; k < 64; ++k) st_bf16(s.at, TILE, k, t, ok ? g[k] : 0.0f);
         st_bf16(s.at, TILE, 64, t, ok ? 1.0f : 0.0f);
         st_bf16(s.dyt, 16, 0, t, dy);
-        // dz3 = dy w4 * silu'(z3)
+        // dz3 = dy w4 * relu'(z3)
 #pragma unroll
-        for (int k = 0; k < 64; ++k) g[k] = dy * s.w4[k] * dsilu(z[k] + s.b3[k]);
+        for (int k = 0; k < 64; ++k) g[k] = dy * s.w4[k] * drelu(z[k] + s.b3[k]);
         store_row64(s.dz, t, g);
 #pragma unroll
         for (int k = 0; k < 64; ++k) st_bf16(s.dzt, MLP_H, k, t, g[k]);
@@ -556,7 +605,7 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict
         // ---- layer 3: dW3 = [h2^T; 1] dz3, dh2 = dz3 W3^T ----
         tc::tmem_ld64(tm + lanebase + TC_Z2, z);
 #pragma unroll
-        for (int k = 0; k < 64; ++k) st_bf16(s.at, TILE, k, t, ok ? silu(z[k] + s.b2[k]) : 0.0f);
+        for (int k = 0; k < 64; ++k) st_bf16(s.at, TILE, k, t, ok ? relu(z[k] + s.b2[k]) : 0.0f);
         good = run_mma(s, phase, err, [&] {
 #pragma unroll
             for (int k = 0; k < 8; ++k)
@@ -569,14 +618,14 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict
         if (!good) break;
         tc::tmem_ld64(tm + lanebase + TC_DH, g);
 #pragma unroll
-        for (int k = 0; k < 64; ++k) g[k] = g[k] * dsilu(z[k] + s.b2[k]);  // dz2 (z holds z2)
+        for (int k = 0; k < 64; ++k) g[k] = g[k] * drelu(z[k] + s.b2[k]);  // dz2 (z holds z2)
         store_row64(s.dz, t, g);
 #pragma unroll
         for (int k = 0; k < 64; ++k) st_bf16(s.dzt, MLP_H, k, t, g[k]);
         // ---- layer 2: dW2 = [h1^T; 1] dz2, dh1 = dz2 W2^T ----
         tc::tmem_ld64(tm + lanebase + TC_Z1, z);
 #pragma unroll
-        for (int k = 0; k < 64; ++k) st_bf16(s.at, TILE, k, t, ok ? silu(z[k] + s.b1[k]) : 0.0f);
+        for (int k = 0; k < 64; ++k) st_bf16(s.at, TILE, k, t, ok ? relu(z[k] + s.b1[k]) : 0.0f);
         good = run_mma(s, phase, err, [&] {
 #pragma unroll
             for (int k = 0; k < 8; ++k)
@@ -589,7 +638,7 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict
         if (!good) break;
         tc::tmem_ld64(tm + lanebase + TC_DH, g);
 #pragma unroll
-        for (int k = 0; k < 64; ++k) g[k] = g[k] * dsilu(z[k] + s.b1[k]);  // dz1 (z holds z1)
+        for (int k = 0; k < 64; ++k) g[k] = g[k] * drelu(z[k] + s.b1[k]);  // dz1 (z holds z1)
 #pragma unroll
         for (int k = 0; k < 64; ++k) st_bf16(s.dzt, MLP_H, k, t, g[k]);
         // ---- layer 1: dW1 = [x^T; 1] dz1 (rows 5..64 of the transposed buffer cleared) ----
@@ -640,10 +689,7 @@ __global__ void __launch_bounds__(TILE, 1) k_mlp_train(const MlpBlob* __restrict
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (t < 32) {
-        tc::tmem_relinquish();
-        tc::tmem_dealloc(tm, TC_NCOL);
-    }
+    if (t < 32) tc::tmem_dealloc(tm, TC_NCOL);
 }
 
 __global__ void k_mlp_adam(float* __restrict__ prm, const float* __restrict__ grad, float* __restrict__ m,
@@ -716,39 +762,32 @@ static int pack(vb_mlp_handle m, cudaStream_t s) {
 
 namespace vb {
 // used by vb_api.cu for the learned-guess stage
-cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const void* Pin, void* Pout, bool fp32,
-                               const double* Uo, unsigned int* err, cudaStream_t s) {
-    LearnedC2PArgs a{};
+cudaError_t launch_mlp_guess(const void* mlp_blob, const StageParams& p, const double* U, float* w_guess,
+                             unsigned int* err, cudaStream_t s) {
+    GuessArgs a{};
     for (int i = 0; i < 3; ++i) a.n[i] = p.n[i];
     a.sy = p.sy;
     a.sz = p.sz;
     a.vs = p.vs;
-    a.gamma = p.gamma;
-    a.floor_ = p.floor_;
-    a.rtol = p.w_rtol;
-    a.max_newton = p.w_max_newton;
-    a.max_bracket = 4 * p.n_iter;
-    a.stats = p.stats;
-    a.Pin_f = fp32 ? (const float*)Pin : nullptr;
-    a.Pin_d = fp32 ? nullptr : (const double*)Pin;
-    a.Pout_f = fp32 ? (float*)Pout : nullptr;
-    a.Pout_d = fp32 ? nullptr : (double*)Pout;
-    a.Uo = Uo;
-    a.counters = p.counters;
+    a.gamma = (float)p.gamma;
+    a.U = U;
+    a.w_guess = w_guess;
     a.err = err;
     static unsigned long long attr = 0;
     int dev = 0;
     cudaGetDevice(&dev);
     if (!(attr >> (dev & 63) & 1ULL)) {
-        cudaError_t e = cudaFuncSetAttribute(k_c2p_learned, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_mlp_guess, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)sizeof(InferSmem));
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k_mlp_guess, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         attr |= 1ULL << (dev & 63);
     }
     const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
-    long long tiles = (cells + TILE - 1) / TILE;
-    int nb = (int)std::min<long long>(tiles, 148LL * 5);
-    k_c2p_learned<<<nb, TILE, sizeof(InferSmem), s>>>((const MlpBlob*)mlp_blob, a);
+    const long long tiles = (cells + TILE - 1) / TILE;
+    const int nb = (int)std::min<long long>(tiles, 148LL * 4);
+    k_mlp_guess<<<nb, TILE, sizeof(InferSmem), s>>>((const MlpBlob*)mlp_blob, a);
     return cudaGetLastError();
 }
 }  // namespace vb
@@ -836,8 +875,9 @@ int vb_mlp_forward(vb_mlp_handle m, const float* feat, int n, float* out, void* 
     if (n == 0) return VB_OK;
     cudaStream_t s = (cudaStream_t)stream;
     MCUDA(m, cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InferSmem)));
+    MCUDA(m, cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     int tiles = (n + TILE - 1) / TILE;
-    k_mlp_forward<<<std::min(tiles, 148 * 5), TILE, sizeof(InferSmem), s>>>(m->blob, feat, n, out, m->err);
+    k_mlp_forward<<<std::min(tiles, 148 * 4), TILE, sizeof(InferSmem), s>>>(m->blob, feat, n, out, m->err);
     MCUDA(m, cudaGetLastError());
     return mlp_check_err(m, s);
 }

@@ -278,13 +278,19 @@ cudaError_t dispatch_stage_zm(int rec, int rs, const StageParams& p, const Stage
 
 // 3D grids whose x/y interior extents are multiples of the z-marching tile
 // use k_stage_zm; everything else (1D, 2D, ragged 3D) the box-tile k_stage.
+// *kernels receives the number of kernels launched (2 for a split z-march
+// stage, whose con2prim runs in k_c2p; else 1).
 template <typename R>
 cudaError_t launch_stage(int dims, int rec, int rs, const StageParams& p, const StageBufs<R>& b,
-                         cudaStream_t s) {
+                         cudaStream_t s, int* kernels) {
+    *kernels = 1;
     if (dims == 1) return dispatch_stage_dim<1, R>(rec, rs, p, b, s);
     if (dims == 2) return dispatch_stage_dim<2, R>(rec, rs, p, b, s);
     if (dims == 3) {
-        if (zm_fits<R>(p) && !p.force_box) return dispatch_stage_zm<R>(rec, rs, p, b, s);
+        if (zm_fits<R>(p) && !p.force_box) {
+            *kernels = p.split && !p.skip_c2p ? 2 : 1;
+            return dispatch_stage_zm<R>(rec, rs, p, b, s);
+        }
         return dispatch_stage_dim<3, R>(rec, rs, p, b, s);
     }
     return cudaErrorInvalidValue;
@@ -551,7 +557,7 @@ cudaError_t launch_max_speed(const Grid& g, const R* P, double gamma, double* pa
 // explicit instantiation of every launcher for one bulk type
 #define VB_INSTANTIATE_LAUNCHERS(R)                                                                      \
     template cudaError_t launch_stage<R>(int, int, int, const StageParams&, const StageBufs<R>&,       \
-                                         cudaStream_t);                                               \
+                                         cudaStream_t, int*);                                         \
     template cudaError_t launch_load_prims<R>(const Grid&, const double*, R*, double*, double,        \
                                               cudaStream_t);                                          \
     template cudaError_t launch_store_prims<R>(const Grid&, const R*, double*, cudaStream_t);        \

@@ -6,4 +6,5 @@
 
 namespace vb {
 VB_INSTANTIATE_LAUNCHERS(float)
+template cudaError_t launch_c2p<float>(const StageParams&, const StageBufs<float>&, cudaStream_t);
 }  // namespace vb

@@ -5,6 +5,7 @@
 
 namespace vb {
 VB_INSTANTIATE_LAUNCHERS(double)
+template cudaError_t launch_c2p<double>(const StageParams&, const StageBufs<double>&, cudaStream_t);
 
 // ---- point kernels: the device physics on arrays of independent states
 // (struct-of-arrays, component k of point i at [k * n + i]) -----------------

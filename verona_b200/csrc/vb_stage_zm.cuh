@@ -334,7 +334,8 @@ template <typename R> inline bool zm_fits(const StageParams& p) {
 }
 
 // Split-mode con2prim: one thread per interior cell, no barriers, no shared
-// memory; reads the stage's U and the guess P, writes the floored P.
+// memory; reads the stage's U and the guess (the stage's input P, or the
+// per-cell W guesses of p.w_guess), writes the floored P.
 template <typename R>
 __global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
     constexpr int NV = 5;
@@ -348,10 +349,11 @@ __global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
         const int k = (int)(e / ((long long)N0 * N1)) + NG;
         const long long c = i + p.sy * j + p.sz * k;
         double U[NV], P[NV];
+        const bool need_p = !(p.c2p_mode == C2P_GUESS_W && p.w_guess);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             U[v] = b.Uo[v * p.vs + c];
-            P[v] = (double)b.Pin[v * p.vs + c];
+            P[v] = need_p ? (double)b.Pin[v * p.vs + c] : 0.0;
         }
         int fb;
         int r = solve_cell<3>(p, U, P, c, fb);
@@ -379,6 +381,13 @@ __global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
     } else if (n_fb) {
         count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
     }
+}
+
+// the split con2prim alone (3D interior), e.g. after a kernel that wrote the W guesses
+template <typename R> cudaError_t launch_c2p(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
+    const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
+    k_c2p<R><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
+    return cudaGetLastError();
 }
 
 template <int REC, int RS, typename R, bool SPLIT>

@@ -52,6 +52,9 @@ __device__ __forceinline__ void tmem_alloc(uint32_t* smem_dst, uint32_t ncols) {
                  "r"(ncols)
                  : "memory");
 }
+// Give up this CTA's right to allocate. Call it right after the CTA's last
+// tcgen05.alloc: while a resident CTA holds the permit, no further CTA of the
+// kernel became resident on its SM (measured: one CTA per SM at a time).
 __device__ __forceinline__ void tmem_relinquish() {
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
 }

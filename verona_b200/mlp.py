@@ -1,9 +1,10 @@
 """Learned con2prim initial guess: training data, training loop and use.
 
-The network (4 -> 64 -> 64 -> 64 -> 1, SiLU, BF16 on the tensor cores with
+The network (4 -> 64 -> 64 -> 64 -> 1, ReLU, BF16 on the tensor cores with
 FP32 accumulation; vb_mlp.cu) maps a conserved state to the pressure guess
 as a fraction of the total energy E = tau + D, y ~ p / E; Newton on
-W = rho h gamma^2 starts from W0 = E (1 + max(y, 0)). Its training pairs are conserved/primitive pairs made by the solver itself:
+W = rho h gamma^2 starts from W0 = E (1 + max(y, 0)). Its training pairs are
+conserved/primitive pairs made by the solver itself:
   * synthetic states with log-uniform rho in [1e-4, 10], log-uniform p/rho in
     [1e-6, 1e2], log-uniform Lorentz factor in [1, 100] in a random direction
     and Gamma in {4/3, 5/3};
@@ -373,3 +374,25 @@ def trained(path=DEFAULT_WEIGHTS, train_if_missing=True, log=None) -> MLP:
 
 def attach(solver, log=None):
     trained(log=log).attach(solver)
+
+
+def main(argv=None):
+    """Train the default network on the current GPU and save it."""
+    import argparse
+    import time
+
+    ap = argparse.ArgumentParser(description="train the learned con2prim guess and save its weights")
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--samples", type=int, default=1 << 22)
+    ap.add_argument("--epochs", type=int, default=4)
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args(argv)
+    t0 = time.time()
+    m = MLP(seed=a.seed)
+    hist = m.train(n_samples=a.samples, epochs=a.epochs, seed=a.seed, log=print)
+    m.save(a.out)
+    print(f"saved {a.out}: {n_params()} parameters, loss per epoch {hist}, {time.time() - t0:.1f} s")
+
+
+if __name__ == "__main__":
+    main()
