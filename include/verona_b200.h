@@ -254,6 +254,51 @@ const char* vb_noalloc_last_error(void);
 int vb_point_c2p_w(double gamma, const double* U, const double* W0, double rtol, int max_newton, int max_bracket,
                    double* P, int* iters, int* fallback, int n, void* stream);
 
+/* ---- batch of independent problems (extension; the reference advances one
+ * grid per HARM_HLL call, src/1dim/algos.jl:58-68, src/2dim/algos.jl:192-208) --
+ * Many 1D and 2D problems of uneven size advance together. Each has its own
+ * interior size, reconstruction, cell widths and time step; all share gamma
+ * and the options' riemann, rk, precision (FP64 or FP32 bulk), n_iter, tol
+ * and floor_ (guess must be VB_GUESS_PREVIOUS), and every face is outflow.
+ * Each problem evolves exactly as a single-grid handle of the same dims and
+ * options with 3 ghost cells would. vb_batch_step runs nsteps steps of every
+ * problem as ONE persistent kernel launch, replayed from a CUDA graph: tiles
+ * (TX2 x TY2 cells in 2D, pencils of L1 cells in 1D) of every RK stage of
+ * every problem are taken in order by the CTAs of one grid, and a tile waits
+ * (bounded) for the previous stage of its own problem only. Tile variants and
+ * CTAs per SM are set by vb_batch_set_tuning (chosen by the Python autotuner,
+ * verona_b200/autotune.py). Arrays are device pointers; the current device is
+ * the handle's. */
+typedef struct {
+    int dims;      /* 1 or 2 */
+    int nx, ny;    /* interior cells (ny = 1 when dims = 1) */
+    int recon;     /* VB_RECON_* */
+    double dx, dy; /* cell widths (dy unused when dims = 1) */
+    double dt;     /* time step */
+} vb_batch_problem;
+typedef struct vb_batch* vb_batch_handle;
+int vb_batch_create(vb_batch_handle* b, int nprob, const vb_batch_problem* probs, double gamma,
+                    const vb_options* o);
+int vb_batch_destroy(vb_batch_handle b);
+const char* vb_batch_last_error(vb_batch_handle b); /* NULL handle: the last failed create */
+/* problem i's primitives, FP64 AoS (2 + dims, nx + 6 [, ny + 6]) as vb_load_prims */
+int vb_batch_load_prims(vb_batch_handle b, int i, const double* P_aos, void* stream);
+int vb_batch_store_prims(vb_batch_handle b, int i, double* P_aos, void* stream);
+int vb_batch_step(vb_batch_handle b, int nsteps, void* stream);
+int vb_batch_get_time(vb_batch_handle b, int i, double* t);
+int vb_batch_get_counters(vb_batch_handle b, uint64_t* out /* VB_CNT_N */, void* stream); /* synchronises */
+int vb_batch_reset_counters(vb_batch_handle b, void* stream);
+/* tile variants of a precision (0 for an invalid precision) and their shapes */
+int vb_batch_num_variants(int precision);
+int vb_batch_variant_shape(int precision, int variant, int* tile_x2, int* tile_y2, int* pencil1);
+/* ctas_per_sm 0: as many as fit; the grid of the last launch is returned by get */
+int vb_batch_set_tuning(vb_batch_handle b, int variant, int ctas_per_sm);
+int vb_batch_get_tuning(vb_batch_handle b, int* variant, int* ctas_per_sm, int* grid);
+int vb_batch_info(vb_batch_handle b, int64_t* interior_cells, int64_t* tiles_per_stage, int64_t* device_bytes);
+/* copy of the state (P, U^n, times) and its restoration, e.g. around tuning runs */
+int vb_batch_checkpoint(vb_batch_handle b, void* stream);
+int vb_batch_rollback(vb_batch_handle b, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

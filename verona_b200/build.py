@@ -7,6 +7,7 @@ Translation units and their floating-point contract:
                                             square root, FTZ (FP32-bulk path; the
                                             FP64 con2prim in it stays IEEE)
   vb_mlp.cu                                 -fmad=true   (BF16 tensor-core MLP)
+  vb_batch_f64.cu / vb_batch_f32.cu         as the FP64 / FP32 stage units (batched problems)
 Objects go to verona_b200/_build/, the library to verona_b200/libverona_b200.so.
 """
 from __future__ import annotations
@@ -67,7 +68,9 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     if os.path.exists(os.path.join(CSRC, "vb_mlp.cu")):
         units["vb_mlp.cu"] = ["-fmad=true"]  # the learned-guess Newton refinement is FP64 with FMA
     if os.path.exists(os.path.join(CSRC, "vb_batch.cu")):
-        units["vb_batch.cu"] = ["-fmad=true"]
+        units["vb_batch.cu"] = ["-fmad=false"]
+        units["vb_batch_f64.cu"] = ["-fmad=false"]
+        units["vb_batch_f32.cu"] = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
     if os.path.exists(os.path.join(CSRC, "vb_noalloc.cu")):
         units["vb_noalloc.cu"] = ["-fmad=false"]
     jobs = jobs or min(len(units), os.cpu_count() or 4)

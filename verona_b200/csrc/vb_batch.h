@@ -1,0 +1,54 @@
+// Batched problems: the launch description shared by the batch kernel
+// (vb_batch.cuh) and its host API (vb_batch.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "vb_internal.h"
+
+namespace vb {
+
+constexpr int BATCH_NT = 256;  // threads per CTA of the batch kernel
+
+struct BatchProb {
+    int dims, rec;
+    int n0, n1;             // padded extents (n1 = 1 in 1D)
+    int ntx, nty;           // tiles per axis (current variant)
+    long long ntiles;
+    long long offP, offU;   // element offset of variable 0 in the P / U pools
+    long long vs;           // variable stride
+    double dtdx[2][2];      // [full dt, half dt (RK2 stage 1)][axis]
+};
+
+struct BatchTile {
+    int p, x, y, pad;
+};
+
+template <typename R> struct BatchLaunch {
+    const BatchProb* prob;
+    const BatchTile* tiles;  // one stage's tiles, largest problems first
+    long long T;             // tiles per stage
+    long long total;         // nsteps * nstages * T
+    int nstages, rk, cur0;   // cur0: P buffer holding the state at the first step
+    int riemann_unused;
+    R* P0;
+    R* P1;
+    double* U0;
+    double* U1;
+    unsigned long long* done;  // per problem
+    unsigned long long* next;  // ticket counter
+    unsigned long long* counters;
+    double gamma, floor_, tol;
+    int n_iter, stats;
+};
+
+// one persistent launch of the batch kernel (instantiated for R = float in
+// vb_batch_f32.cu and R = double in vb_batch_f64.cu); *grid receives the CTA
+// count. launch = false only sets the kernel attributes and computes the grid.
+template <typename R>
+cudaError_t batch_launch(const BatchLaunch<R>& a, int riemann, int variant, int ctas_per_sm, cudaStream_t s,
+                         int* grid, bool launch);
+// number of tile-shape variants and the shape of one: 2D tile TX2 x TY2, 1D pencil L1
+template <typename R> int batch_num_variants();
+template <typename R> void batch_variant_shape(int v, int* tx2, int* ty2, int* l1);
+
+}  // namespace vb

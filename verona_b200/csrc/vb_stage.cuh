@@ -70,21 +70,29 @@ __device__ __forceinline__ int solve_cell(const StageParams& p, const double* U,
     return r;
 }
 
-template <int DIM, int REC, int RS, typename R, int TX, int TY, int TZ, int NT>
-__global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
+// Loads of the stage inputs. CG: through L2 only (ld.global.cg), for a kernel
+// that reads arrays written earlier in the same launch by other CTAs.
+template <bool CG, typename T> __device__ __forceinline__ T ld_in(const T* p) {
+    if (CG) return __ldcg(p);
+    return *p;
+}
+
+// One TX x TY x TZ tile of a stage (tile coordinates bx, by, bz); the body of
+// k_stage, shared with the batched kernel. smem_raw: TileGeom::smem_bytes<R>().
+template <int DIM, int REC, int RS, typename R, int TX, int TY, int TZ, int NT, bool CG>
+__device__ __forceinline__ void stage_tile(const StageParams& p, const StageBufs<R>& b, int bx, int by, int bz,
+                                           unsigned char* smem_raw) {
     using G = TileGeom<DIM, TX, TY, TZ>;
     constexpr int NV = G::NV;
     constexpr int TC = G::TC;
     constexpr int CPT = (TC + NT - 1) / NT;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     R* sP = reinterpret_cast<R*>(smem_raw);
     R* sL = sP + NV * G::EXTMAX;
     R* sR = sL + NV * G::FACEMAX;
 
     const int tid = threadIdx.x;
     const int T[3] = {TX, TY, TZ};
-    const int org[3] = {NG + (int)blockIdx.x * TX, DIM > 1 ? NG + (int)blockIdx.y * TY : 0,
-                        DIM > 2 ? NG + (int)blockIdx.z * TZ : 0};
+    const int org[3] = {NG + bx * TX, DIM > 1 ? NG + by * TY : 0, DIM > 2 ? NG + bz * TZ : 0};
     // valid cells of this (possibly partial) tile along each axis
     int vt[3];
     #pragma unroll
@@ -101,7 +109,7 @@ __global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
         bool ok = cell < TC && lx < vt[0] && ly < vt[1] && lz < vt[2];
         long long gidx = (org[0] + lx) + p.sy * (org[1] + ly) + p.sz * (org[2] + lz);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) acc[c][v] = ok ? b.Us[v * vs + gidx] : 0.0;
+        for (int v = 0; v < NV; ++v) acc[c][v] = ok ? ld_in<CG>(b.Us + v * vs + gidx) : 0.0;
     }
 
 #pragma unroll 1
@@ -117,7 +125,7 @@ __global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
             int ex = r % EX, ey = (r / EX) % EY, ez = r / (EX * EY);
             int gi = ox + ex, gj = oy + ey, gk = oz + ez;
             R val = R(0);
-            if (gi < p.n[0] && gj < p.n[1] && gk < p.n[2]) val = b.Pin[v * vs + gi + p.sy * gj + p.sz * gk];
+            if (gi < p.n[0] && gj < p.n[1] && gk < p.n[2]) val = ld_in<CG>(b.Pin + v * vs + gi + p.sy * gj + p.sz * gk);
             sP[v * EXT + r] = val;
         }
         __syncthreads();
@@ -175,7 +183,7 @@ __global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
         }
         __syncthreads();
         // 4. flux difference, in the reference's order x, y, z
-        const double cdt = p.dtdx[d];
+        const double cdt = d == 0 ? p.dtdx[0] : (d == 1 ? p.dtdx[1] : p.dtdx[2]);
         const int fstep = d == 0 ? 1 : (d == 1 ? FX : FX * FY);
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
@@ -201,10 +209,10 @@ __global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             double u = acc[c][v];
-            if (p.rk_a != 0.0) u = p.rk_a * b.U0[v * vs + gidx] + p.rk_b * u;
+            if (p.rk_a != 0.0) u = p.rk_a * ld_in<CG>(b.U0 + v * vs + gidx) + p.rk_b * u;
             U[v] = u;
             b.Uo[v * vs + gidx] = u;
-            P[v] = (double)b.Pin[v * vs + gidx];
+            P[v] = (double)ld_in<CG>(b.Pin + v * vs + gidx);
         }
         if (p.skip_c2p) continue;  // con2prim runs in a separate kernel
         int fb;
@@ -234,6 +242,13 @@ __global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
     } else if (n_fb) {
         count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
     }
+}
+
+template <int DIM, int REC, int RS, typename R, int TX, int TY, int TZ, int NT>
+__global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    stage_tile<DIM, REC, RS, R, TX, TY, TZ, NT, false>(p, b, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z,
+                                                       smem_raw);
 }
 
 template <int DIM, int REC, int RS, typename R>
