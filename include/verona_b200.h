@@ -254,6 +254,35 @@ const char* vb_noalloc_last_error(void);
 int vb_point_c2p_w(double gamma, const double* U, const double* W0, double rtol, int max_newton, int max_bracket,
                    double* P, int* iters, int* fallback, int n, void* stream);
 
+/* ---- grid kernels one at a time (the reference's kernels as separate calls) ------
+ * Caller-owned device arrays in the reference layout: FP64 AoS (2 + dims,
+ * nx+6 [, ny+6 [, nz+6]]), variable fastest. For a caller that replaces single
+ * kernels of HARM_HLL; the fused time loop is vb_step. FP64, bit-identical to
+ * the reference's arithmetic. Errors: vb_grid_last_error().
+ *   fluxes:   function_Fluxes of one axis (src/3dim/algos.jl:14-176,
+ *             src/2dim/algos.jl:11-168): face i+1/2 into F[:, i] for every index
+ *             in [2, n+2] (0-based, padded) on all active axes; face states are
+ *             reconstructed with `recon`, floored at floor_, then the Riemann flux
+ *   update:   function_Update (src/3dim/algos.jl:178-200): interior cells,
+ *             Uout = U - dt/dx (Fx_i - Fx_{i-1}) - dt/dy (...) - dt/dz (...)
+ *   con2prim: function_UtoP (src/3dim/structs.jl:218-628, src/2dim/structs.jl:249-330,
+ *             src/1dim/structs.jl:78-105) on interior cells, P in: guess, out:
+ *             primitives (NaN where no root); failures_dev (may be NULL) counts the
+ *             cells where every stage gave up (a 3D stage that converges to a
+ *             non-finite state also leaves NaN, as in the reference)
+ *   prim2con: kernel_PtoU (src/3dim/structs.jl:66-81) on all cells
+ *   limit:    function_Limit (src/3dim/algos.jl:5-12) on all cells */
+int vb_grid_fluxes(int dims, int nx, int ny, int nz, const double* P_aos, double gamma, double floor_, int axis,
+                   int recon, int riemann, double* F_aos, void* stream);
+int vb_grid_update(int dims, int nx, int ny, int nz, const double* U_aos, const double* Fx, const double* Fy,
+                   const double* Fz, double dt, double dx, double dy, double dz, double* Uout_aos, void* stream);
+int vb_grid_con2prim(int dims, int nx, int ny, int nz, const double* U_aos, double gamma, int n_iter, double tol,
+                     double* P_aos, uint64_t* failures_dev, void* stream);
+int vb_grid_prim2con(int dims, int nx, int ny, int nz, const double* P_aos, double gamma, double* U_aos,
+                     void* stream);
+int vb_grid_limit(int dims, int nx, int ny, int nz, double* P_aos, double floor_, void* stream);
+const char* vb_grid_last_error(void);
+
 /* ---- batch of independent problems (extension; the reference advances one
  * grid per HARM_HLL call, src/1dim/algos.jl:58-68, src/2dim/algos.jl:192-208) --
  * Many 1D and 2D problems of uneven size advance together. Each has its own

@@ -82,3 +82,21 @@ def test_create_rejects_bad_options_without_a_gpu():
     o.version = 99
     assert L.vb_create(C.byref(h), 2, 8, 8, 1, 3, C.byref(o)) == _lib.ERR_ARG
     assert L.vb_step(None, 0.1, 1, None) == _lib.ERR_ARG
+
+
+def test_grid_entry_points_reject_bad_arguments_without_a_gpu():
+    import ctypes as C
+
+    from verona_b200 import _lib as L
+
+    lib = L.lib()
+    vp, d, i = C.c_void_p, C.c_double, C.c_int
+    lib.vb_grid_fluxes.argtypes = [i, i, i, i, vp, d, d, i, i, i, vp, vp]
+    lib.vb_grid_limit.argtypes = [i, i, i, i, vp, d, vp]
+    lib.vb_grid_last_error.restype = C.c_char_p
+    assert lib.vb_grid_fluxes(2, 8, 8, 1, None, 4 / 3, 1e-8, 0, 2, 1, None, None) == L.ERR_ARG
+    assert b"null" in lib.vb_grid_last_error()
+    assert lib.vb_grid_fluxes(2, 8, 8, 1, C.c_void_p(16), 4 / 3, 1e-8, 2, 2, 1, C.c_void_p(16), None) == L.ERR_ARG
+    assert b"axis 2" in lib.vb_grid_last_error()
+    assert lib.vb_grid_limit(4, 8, 8, 8, None, 0.0, None) == L.ERR_ARG
+    assert b"dims 4" in lib.vb_grid_last_error()

@@ -71,6 +71,8 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         units["vb_batch.cu"] = ["-fmad=false"]
         units["vb_batch_f64.cu"] = ["-fmad=false"]
         units["vb_batch_f32.cu"] = ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
+    if os.path.exists(os.path.join(CSRC, "vb_grid.cu")):
+        units["vb_grid.cu"] = ["-fmad=false"]
     if os.path.exists(os.path.join(CSRC, "vb_noalloc.cu")):
         units["vb_noalloc.cu"] = ["-fmad=false"]
     jobs = jobs or min(len(units), os.cpu_count() or 4)
