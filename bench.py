@@ -51,6 +51,8 @@ def parse():
                     help="fp64: time only the plain FP64 path (profiling runs)")
     ap.add_argument("--guess", default="auto", choices=["auto", "learned", "previous"],
                     help="con2prim guess of the fast path (auto: learned when the network is available)")
+    ap.add_argument("--learned-form", default="fused", choices=["fused", "two"],
+                    help="learned con2prim as one kernel (guess + Newton) or as a guess kernel + con2prim kernel")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default="jet3d", choices=["jet3d", "batch"],
                     help="batch: 256 uneven 1D/2D Riemann problems in one persistent launch (not the headline)")
@@ -321,6 +323,7 @@ def run_ours(args, rank, world, dist):
     s = make_solver(n, "fp32", guess)
     if learned_ok:
         mlp.attach(s)
+        s.set_tuning(learned_fused=int(args.learned_form == "fused"))
     s.load_prims(P0)
     with Clocks(torch.cuda.current_device()) as clk:
         ms, st_ms, st_l, launches = timed_steps(s, dt, W, K, dist)
@@ -374,12 +377,13 @@ def run_ours(args, rank, world, dist):
     bytes_per_cell_step = 440.0
     stage_ms_per_launch = st_ms / max(st_l, 1)
     achieved = cells * bytes_per_cell_step / 3.0 / (stage_ms_per_launch / 1e3) / 1e9
-    traffic = read_traffic(f"fp32_{guess}_stage_group")
+    form = "_fused" if learned_ok and args.learned_form == "fused" else ""
+    traffic = read_traffic(f"fp32_{guess}{form}_stage_group")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 bulk + f64 (U, con2prim)", "data": "synthetic",
-        "config": workload_config(n, guess),
+        "config": dict(workload_config(n, guess), learned_form=args.learned_form if learned_ok else None),
         "fp64_plain": fp64,
         "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
         "l1_error_vs_fp64": err,

@@ -152,11 +152,16 @@ int vb_reset_counters(vb_handle h, void* stream);
  * split_con2prim: 1 = the 3D stencil kernel writes U and a separate
  * barrier-free kernel solves con2prim; 0 = one fused kernel; -1 = library
  * default. force_box: 1 = use the box-tile stencil kernel for 3D even where
- * the z-marching kernel fits. Results are identical for every variant. */
+ * the z-marching kernel fits. Results are identical for every variant.
+ * learned_fused (guess = VB_GUESS_LEARNED only): 1 = the network's guess and
+ * the W Newton from it run in one kernel; 0 = a guess kernel writes one W per
+ * cell and the con2prim kernel reads it; -1 = library default (1). Both start
+ * the Newton from the same FP32-rounded guess. */
 typedef struct vb_tuning {
     int32_t split_con2prim;
     int32_t force_box;
-    int32_t reserved[6];
+    int32_t learned_fused;
+    int32_t reserved[5];
 } vb_tuning;
 int vb_set_tuning(vb_handle h, const vb_tuning* t);
 int vb_get_tuning(vb_handle h, vb_tuning* t);

@@ -147,3 +147,38 @@ def test_learned_solver_matches_fp64_path(net):
     assert c[0] == 0 and c[4] == 0
     assert max(per_field_rel(out["learned"][1], out["previous"][1])) < 1e-9
     assert max(per_field_rel(out["learned"][0], out["previous"][0])) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_learned_fused_kernel_matches_two_kernel_form(net, precision):
+    """The one-kernel learned con2prim (guess + W Newton per 128-cell tile)
+    against the guess kernel + con2prim kernel pair: both start each cell's
+    Newton from the same FP32-rounded network guess, so they agree to the
+    Newton tolerance (the two forms are built in different compilation units,
+    whose FP64 contraction may differ in the last bit)."""
+    from helpers import jet_ic, nozzle_params, per_field_rel
+    from verona_b200 import Solver
+
+    n = (32, 16, 24)
+    P0 = jet_ic(3, n, gamma=G, noise=0.03, seed=5)
+    dxs = [1.0 / 32] * 3
+    dt = 0.4 / sum(1.0 / d for d in dxs)
+    out = {}
+    for fused in (0, 1):
+        s = Solver(3, n, G, dxs, recon="wenoz", riemann="hllc", rk=3, guess="learned", precision=precision,
+                   n_iter=50, tol=1e-12, floor=1e-8, stats=1)
+        net.attach(s)
+        s.set_tuning(learned_fused=fused)
+        assert s.get_tuning()["learned_fused"] == fused
+        s.set_boundary(0, 2, nozzle_params(3, n, 4.0, gamma=G))
+        s.load_prims(P0)
+        s.step(dt, 5)
+        out[fused] = (s.prims(), s.cons(), s.counters())
+    c0, c1 = out[0][2], out[1][2]
+    print(precision, "two-kernel counters", c0.tolist(), "fused", c1.tolist())
+    assert c1[0] == 0 and c1[4] == 0 and c1[3] == c0[3]
+    assert abs(int(c1[2]) - int(c0[2])) <= 0.01 * int(c0[2])
+    ep = max(per_field_rel(out[1][0], out[0][0]))
+    eu = max(per_field_rel(out[1][1], out[0][1]))
+    print(precision, "fused vs two-kernel: max rel diff P %.3e U %.3e" % (ep, eu))
+    assert eu < 1e-9 and ep < 1e-8

@@ -53,7 +53,7 @@ struct vb_solver {
     size_t bytes = 0;
     std::string err;
     // kernel variants
-    vb_tuning tun{-1, 0, {0, 0, 0, 0, 0, 0}};
+    vb_tuning tun{-1, 0, -1, {0, 0, 0, 0, 0}};
     // learned con2prim guess
     const void* mlp_blob = nullptr;
     unsigned int* tc_err = nullptr;
@@ -433,13 +433,18 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
         VB_CUDA(h, launch_stage<R>(h->dims, h->opt.recon, h->opt.riemann, p, bufs, s, &nk));
         if (p.skip_c2p) {
             // learned guess: the network's W per cell, then the W Newton from it
-            VB_CUDA(h, launch_mlp_guess(h->mlp_blob, p, Uo, h->w_guess, h->tc_err, s));
             StageParams q = p;
             q.skip_c2p = 0;
             q.c2p_mode = C2P_GUESS_W;
-            q.w_guess = h->w_guess;
-            VB_CUDA(h, launch_c2p<R>(q, bufs, s));
-            h->launches += 2;
+            if (h->tun.learned_fused != 0) {
+                VB_CUDA(h, launch_c2p_learned<R>(h->mlp_blob, q, Uo, Pout, h->tc_err, s));
+                h->launches += 1;
+            } else {
+                VB_CUDA(h, launch_mlp_guess(h->mlp_blob, p, Uo, h->w_guess, h->tc_err, s));
+                q.w_guess = h->w_guess;
+                VB_CUDA(h, launch_c2p<R>(q, bufs, s));
+                h->launches += 2;
+            }
         }
         if (h->prof) VB_CUDA(h, cudaEventRecord(e1, s));
         VB_CUDA(h, launch_ghost_limit<R>(g, Pin, Pout, h->opt.floor_, s));
@@ -575,8 +580,10 @@ int vb_attach_mlp(vb_handle h, vb_mlp_handle m) {
 
 int vb_set_tuning(vb_handle h, const vb_tuning* t) {
     if (!h || !t) return fail(h, VB_ERR_ARG, "vb_set_tuning: null argument");
-    if (t->split_con2prim < -1 || t->split_con2prim > 1 || t->force_box < 0 || t->force_box > 1)
-        return fail(h, VB_ERR_ARG, "vb_set_tuning: split_con2prim in {-1,0,1}, force_box in {0,1}");
+    if (t->split_con2prim < -1 || t->split_con2prim > 1 || t->force_box < 0 || t->force_box > 1 ||
+        t->learned_fused < -1 || t->learned_fused > 1)
+        return fail(h, VB_ERR_ARG,
+                    "vb_set_tuning: split_con2prim in {-1,0,1}, force_box in {0,1}, learned_fused in {-1,0,1}");
     h->tun = *t;
     return VB_OK;
 }

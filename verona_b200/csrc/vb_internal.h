@@ -97,6 +97,11 @@ template <typename R> cudaError_t launch_c2p(const StageParams& p, const StageBu
 // (padded SoA, the grid of p) into w_guess (one float per padded cell)
 cudaError_t launch_mlp_guess(const void* mlp_blob, const StageParams& p, const double* U, float* w_guess,
                              unsigned int* err, cudaStream_t s);
+// the same guess and the W Newton from it in one kernel (vb_mlp.cu): U of the
+// stage in, the floored P of every interior cell out
+template <typename R>
+cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const double* U, R* Pout,
+                               unsigned int* err, cudaStream_t s);
 
 // point kernels (FP64, vb_stage_f64.cu)
 cudaError_t launch_point_recon(int method, const double* q, double* out, int n, cudaStream_t s);

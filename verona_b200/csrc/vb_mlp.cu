@@ -790,6 +790,128 @@ cudaError_t launch_mlp_guess(const void* mlp_blob, const StageParams& p, const d
     k_mlp_guess<<<nb, TILE, sizeof(InferSmem), s>>>((const MlpBlob*)mlp_blob, a);
     return cudaGetLastError();
 }
+
+// ---- fused learned con2prim of a split stage ------------------------------------------
+// k_mlp_guess followed by k_c2p in one persistent kernel: per 128-cell tile,
+// U is read once, the network's W0 stays in the thread that runs the W Newton
+// from it (no W guess array in HBM), and the Newton's FP64 work of the other
+// CTAs on the SM overlaps each CTA's MMA round trips. W0 is rounded to FP32
+// exactly as the two-kernel form stores it, so both forms start the Newton
+// from the same guess.
+template <typename R>
+__global__ void __launch_bounds__(TILE, 4) k_c2p_learned(const MlpBlob* __restrict__ blob, StageParams p,
+                                                         const double* __restrict__ U, R* __restrict__ Pout,
+                                                         unsigned int* err) {
+    extern __shared__ __align__(128) unsigned char smraw[];
+    InferSmem& s = *reinterpret_cast<InferSmem*>(smraw);
+    const int t = threadIdx.x;
+    infer_begin(s, blob);
+    const int N0 = p.n[0] - 2 * NG, N1 = p.n[1] - 2 * NG, N2 = p.n[2] - 2 * NG;
+    const long long tot = (long long)N0 * N1 * N2;
+    const long long ntiles = (tot + TILE - 1) / TILE;
+    const long long vs = p.vs;
+    auto cell = [&](long long e, long long& c) -> bool {
+        if (e >= tot) return false;
+        const int i = (int)(e % N0) + NG;
+        const int j = (int)((e / N0) % N1) + NG;
+        const int k = (int)(e / ((long long)N0 * N1)) + NG;
+        c = i + p.sy * j + p.sz * k;
+        return true;
+    };
+    unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
+    uint32_t phase = 0;
+    long long tile = blockIdx.x;
+    long long c = 0;
+    bool ok = tile < ntiles && cell(tile * TILE + t, c);
+    double u[5] = {1.0, -2.0, 0.0, 0.0, 0.0};
+    if (ok)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) u[v] = U[v * vs + c];
+    for (; tile < ntiles; tile += gridDim.x) {
+        const long long nt = tile + gridDim.x;
+        long long cn = 0;
+        const bool okn = nt < ntiles && cell(nt * TILE + t, cn);
+        double un[5] = {1.0, -2.0, 0.0, 0.0, 0.0};
+        if (okn)
+#pragma unroll
+            for (int v = 0; v < 5; ++v) un[v] = U[v * vs + cn];
+        float f[4];
+        guess_features(u, (float)p.gamma, s.mu, s.isd, f);
+        float y = 0.f;
+        if (!mlp_forward_tile(s, f, y, phase, err)) break;
+        if (ok) {
+            const double W0 = (double)(float)(-u[1] * (1.0 + (double)fmaxf(y, 0.0f)));
+            double P[5];
+            int fb;
+            const int r = c2p_w(p.gamma, u, W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, P, &fb);
+            n_fail += (r < 0);
+            n_fb += fb;
+            n_it += (r < 0 ? -r : r);
+            n_cells += 1;
+            P[0] = jmax(P[0], p.floor_);
+            P[1] = jmax(P[1], p.floor_);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) Pout[v * vs + c] = (R)P[v];
+        }
+        ok = okn;
+        c = cn;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) u[v] = un[v];
+    }
+    infer_end(s);
+    unsigned long long* cnt = p.counters;
+    if (!cnt) return;
+    if (n_fail) atomicAdd(cnt + CNT_C2P_FAIL, n_fail);
+    if (p.stats) {
+        for (int o = 16; o > 0; o >>= 1) {
+            n_fb += __shfl_xor_sync(0xffffffffu, n_fb, o);
+            n_it += __shfl_xor_sync(0xffffffffu, n_it, o);
+            n_cells += __shfl_xor_sync(0xffffffffu, n_cells, o);
+        }
+        if ((t & 31) == 0) {
+            if (n_fb) atomicAdd(cnt + CNT_C2P_FALLBACK, n_fb);
+            if (n_it) atomicAdd(cnt + CNT_C2P_ITERS, n_it);
+            if (n_cells) atomicAdd(cnt + CNT_C2P_CELLS, n_cells);
+        }
+    } else if (n_fb) {
+        atomicAdd(cnt + CNT_C2P_FALLBACK, n_fb);
+    }
+}
+
+template <typename R>
+cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const double* U, R* Pout,
+                               unsigned int* err, cudaStream_t s) {
+    static unsigned long long attr = 0;
+    static int resident[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int d = dev & 63;
+    if (!(attr >> d & 1ULL)) {
+        cudaError_t e = cudaFuncSetAttribute(k_c2p_learned<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(InferSmem));
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k_c2p_learned<R>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
+        // 4 CTAs per SM: the launch bound (128 registers x 128 threads), 4 x 47 KB of
+        // shared memory and 4 x 64 TMEM columns all fit (the occupancy query
+        // reported 1 per SM here, which left the SM idle during each MMA round trip)
+        int sms = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        resident[d] = 4 * std::max(1, sms);
+        attr |= 1ULL << d;
+    }
+    const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
+    const long long tiles = (cells + TILE - 1) / TILE;
+    const int nb = (int)std::min<long long>(tiles, resident[d]);
+    if (nb <= 0) return cudaSuccess;
+    k_c2p_learned<R><<<nb, TILE, sizeof(InferSmem), s>>>((const MlpBlob*)mlp_blob, p, U, Pout, err);
+    return cudaGetLastError();
+}
+template cudaError_t launch_c2p_learned<float>(const void*, const StageParams&, const double*, float*,
+                                               unsigned int*, cudaStream_t);
+template cudaError_t launch_c2p_learned<double>(const void*, const StageParams&, const double*, double*,
+                                                unsigned int*, cudaStream_t);
 }  // namespace vb
 
 extern "C" {
