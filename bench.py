@@ -53,6 +53,8 @@ def parse():
                     help="con2prim guess of the fast path (auto: learned when the network is available)")
     ap.add_argument("--learned-form", default="fused", choices=["fused", "two"],
                     help="learned con2prim as one kernel (guess + Newton) or as a guess kernel + con2prim kernel")
+    ap.add_argument("--stencil", default="pairs", choices=["pairs", "scalar"],
+                    help="FP32 stencil kernel: two cells per thread on packed FP32 pairs, or one cell per thread")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--workload", default="jet3d", choices=["jet3d", "batch"],
                     help="batch: 256 uneven 1D/2D Riemann problems in one persistent launch (not the headline)")
@@ -323,7 +325,7 @@ def run_ours(args, rank, world, dist):
     s = make_solver(n, "fp32", guess)
     if learned_ok:
         mlp.attach(s)
-        s.set_tuning(learned_fused=int(args.learned_form == "fused"))
+    s.set_tuning(learned_fused=int(args.learned_form == "fused"), fp32_pairs=int(args.stencil == "pairs"))
     s.load_prims(P0)
     with Clocks(torch.cuda.current_device()) as clk:
         ms, st_ms, st_l, launches = timed_steps(s, dt, W, K, dist)
@@ -383,7 +385,8 @@ def run_ours(args, rank, world, dist):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 bulk + f64 (U, con2prim)", "data": "synthetic",
-        "config": dict(workload_config(n, guess), learned_form=args.learned_form if learned_ok else None),
+        "config": dict(workload_config(n, guess), learned_form=args.learned_form if learned_ok else None,
+                       stencil=args.stencil),
         "fp64_plain": fp64,
         "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
         "l1_error_vs_fp64": err,

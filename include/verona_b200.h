@@ -156,12 +156,17 @@ int vb_reset_counters(vb_handle h, void* stream);
  * learned_fused (guess = VB_GUESS_LEARNED only): 1 = the network's guess and
  * the W Newton from it run in one kernel; 0 = a guess kernel writes one W per
  * cell and the con2prim kernel reads it; -1 = library default (1). Both start
- * the Newton from the same FP32-rounded guess. */
+ * the Newton from the same FP32-rounded guess.
+ * fp32_pairs (precision = VB_PREC_FP32_BULK, 3D, WENOZ with HLL or HLLC): 1 =
+ * the z-pair stencil kernel (two cells per thread on packed FP32 pairs);
+ * 0 = one cell per thread; -1 = library default (1). The two agree to FP32
+ * rounding, not bitwise. */
 typedef struct vb_tuning {
     int32_t split_con2prim;
     int32_t force_box;
     int32_t learned_fused;
-    int32_t reserved[5];
+    int32_t fp32_pairs;
+    int32_t reserved[4];
 } vb_tuning;
 int vb_set_tuning(vb_handle h, const vb_tuning* t);
 int vb_get_tuning(vb_handle h, vb_tuning* t);

@@ -155,7 +155,10 @@ def test_learned_fused_kernel_matches_two_kernel_form(net, precision):
     against the guess kernel + con2prim kernel pair: both start each cell's
     Newton from the same FP32-rounded network guess, so they agree to the
     Newton tolerance (the two forms are built in different compilation units,
-    whose FP64 contraction may differ in the last bit)."""
+    whose FP64 contraction may differ in the last bit). Both run the
+    one-cell-per-thread FP32 stencil kernel here; the z-pair stencil, which
+    leaves the divergence for the fused kernel to combine, is compared with it
+    at FP32 rounding."""
     from helpers import jet_ic, nozzle_params, per_field_rel
     from verona_b200 import Solver
 
@@ -164,16 +167,16 @@ def test_learned_fused_kernel_matches_two_kernel_form(net, precision):
     dxs = [1.0 / 32] * 3
     dt = 0.4 / sum(1.0 / d for d in dxs)
     out = {}
-    for fused in (0, 1):
+    for fused, pairs in ((0, 0), (1, 0), (1, 1)):
         s = Solver(3, n, G, dxs, recon="wenoz", riemann="hllc", rk=3, guess="learned", precision=precision,
                    n_iter=50, tol=1e-12, floor=1e-8, stats=1)
         net.attach(s)
-        s.set_tuning(learned_fused=fused)
+        s.set_tuning(learned_fused=fused, fp32_pairs=pairs)
         assert s.get_tuning()["learned_fused"] == fused
         s.set_boundary(0, 2, nozzle_params(3, n, 4.0, gamma=G))
         s.load_prims(P0)
         s.step(dt, 5)
-        out[fused] = (s.prims(), s.cons(), s.counters())
+        out[fused + pairs] = (s.prims(), s.cons(), s.counters())
     c0, c1 = out[0][2], out[1][2]
     print(precision, "two-kernel counters", c0.tolist(), "fused", c1.tolist())
     assert c1[0] == 0 and c1[4] == 0 and c1[3] == c0[3]
@@ -182,3 +185,9 @@ def test_learned_fused_kernel_matches_two_kernel_form(net, precision):
     eu = max(per_field_rel(out[1][1], out[0][1]))
     print(precision, "fused vs two-kernel: max rel diff P %.3e U %.3e" % (ep, eu))
     assert eu < 1e-9 and ep < 1e-8
+    c2 = out[2][2]
+    assert c2[0] == 0 and c2[4] == 0
+    a, b = out[2][0][:, 3:-3, 3:-3, 3:-3], out[1][0][:, 3:-3, 3:-3, 3:-3]
+    l1 = [float(np.mean(np.abs(a[v] - b[v])) / np.mean(np.abs(b[v]))) for v in (0, 1)]
+    print(precision, "z-pair stencil + fused vs one-cell stencil + fused: L1 rho, p", l1)
+    assert max(l1) < (1e-12 if precision == "fp64" else 2e-6)

@@ -282,3 +282,44 @@ def test_zmarch_kernel_parity(oracle, rec, rs, rk, variant):
     eP = per_field_rel(got, ref)
     print("zm", rec, rs, rk, "U", max(eU), "P", max(eP), "differing", int(np.sum(got != ref)))
     assert max(eU) <= TOL and max(eP) <= TOL
+
+
+@pytest.mark.parametrize("rs", ["hll", "hllc"])
+@pytest.mark.parametrize("variant", ["split", "fused"])
+def test_fp32_pair_kernel_matches_scalar_kernel(rs, variant):
+    """The z-pair FP32 stencil kernel (two cells per thread on packed FP32
+    instructions) against the one-cell-per-thread FP32 kernel and the FP64
+    path. 69 cells in z give a 64-cell range and a 5-cell range, whose last
+    pair is incomplete. The two FP32 kernels round differently (hand-written
+    packed contraction, folded constants), so they agree to FP32 rounding, and
+    each stays within the FP32-bulk error bar of the FP64 run."""
+    from verona_b200 import Solver
+
+    g = 4.0 / 3.0
+    n = (32, 16, 69)
+    P0 = jet_ic(3, n, gamma=g, noise=0.03, seed=8)
+    dxs = [1.0 / 32] * 3
+    dt = 0.4 / sum(1.0 / d for d in dxs)
+    out = {}
+    for name, prec, pairs in (("fp64", "fp64", 0), ("scalar", "fp32", 0), ("pairs", "fp32", 1)):
+        s = Solver(3, n, g, dxs, recon="wenoz", riemann=rs, rk=3, precision=prec, n_iter=50, tol=1e-12, floor=1e-8)
+        s.set_tuning(split_con2prim=int(variant == "split"), fp32_pairs=pairs)
+        s.set_boundary(0, 2, nozzle_params(3, n, 5.0, gamma=g))
+        s.load_prims(P0)
+        s.step(dt, 6)
+        out[name] = s.prims()[:, 3:-3, 3:-3, 3:-3]
+        assert s.counters()[0] == 0
+        assert np.all(np.isfinite(out[name]))
+
+    def l1(a, b, v):
+        return float(np.mean(np.abs(a[v] - b[v])) / np.mean(np.abs(b[v])))
+
+    for v in range(5):
+        d = l1(out["pairs"], out["scalar"], v) if v < 2 else float(
+            np.mean(np.abs(out["pairs"][v] - out["scalar"][v])))
+        print(rs, variant, "var", v, "pairs vs scalar FP32:", d)
+        assert d < 2e-6
+    for name in ("scalar", "pairs"):
+        e = (l1(out[name], out["fp64"], 0), l1(out[name], out["fp64"], 1))
+        print(rs, variant, name, "L1 rho, p vs FP64:", e)
+        assert max(e) < 1e-5

@@ -53,7 +53,7 @@ struct vb_solver {
     size_t bytes = 0;
     std::string err;
     // kernel variants
-    vb_tuning tun{-1, 0, -1, {0, 0, 0, 0, 0}};
+    vb_tuning tun{-1, 0, -1, -1, {0, 0, 0, 0}};
     // learned con2prim guess
     const void* mlp_blob = nullptr;
     unsigned int* tc_err = nullptr;
@@ -414,9 +414,13 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
     p.force_box = h->tun.force_box;
     p.split = h->tun.split_con2prim < 0 ? default_split(h) : h->tun.split_con2prim;
     p.skip_c2p = 0;
+    p.pairs = h->tun.fp32_pairs != 0;
     if (h->opt.guess == VB_GUESS_LEARNED) {
         if (!h->mlp_blob) return fail(h, VB_ERR_STATE, "vb_step: guess = LEARNED needs vb_attach_mlp");
         p.skip_c2p = 1;
+        // the fused learned con2prim forms U from the divergence; the separate
+        // guess kernel of the two-kernel form reads a formed U
+        p.want_div = h->tun.learned_fused != 0;
     }
     auto stage = [&](const R* Pin, R* Pout, const double* Us, double* Uo, double dts, double a, double b) -> int {
         for (int d = 0; d < 3; ++d) p.dtdx[d] = d < h->dims ? dts / h->dx[d] : 0.0;
@@ -436,8 +440,9 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
             StageParams q = p;
             q.skip_c2p = 0;
             q.c2p_mode = C2P_GUESS_W;
+            q.div_in_pout = stage_div_in_pout<R>(h->dims, h->opt.recon, h->opt.riemann, p);
             if (h->tun.learned_fused != 0) {
-                VB_CUDA(h, launch_c2p_learned<R>(h->mlp_blob, q, Uo, Pout, h->tc_err, s));
+                VB_CUDA(h, launch_c2p_learned<R>(h->mlp_blob, q, bufs, h->tc_err, s));
                 h->launches += 1;
             } else {
                 VB_CUDA(h, launch_mlp_guess(h->mlp_blob, p, Uo, h->w_guess, h->tc_err, s));
@@ -581,9 +586,10 @@ int vb_attach_mlp(vb_handle h, vb_mlp_handle m) {
 int vb_set_tuning(vb_handle h, const vb_tuning* t) {
     if (!h || !t) return fail(h, VB_ERR_ARG, "vb_set_tuning: null argument");
     if (t->split_con2prim < -1 || t->split_con2prim > 1 || t->force_box < 0 || t->force_box > 1 ||
-        t->learned_fused < -1 || t->learned_fused > 1)
+        t->learned_fused < -1 || t->learned_fused > 1 || t->fp32_pairs < -1 || t->fp32_pairs > 1)
         return fail(h, VB_ERR_ARG,
-                    "vb_set_tuning: split_con2prim in {-1,0,1}, force_box in {0,1}, learned_fused in {-1,0,1}");
+                    "vb_set_tuning: split_con2prim in {-1,0,1}, force_box in {0,1}, learned_fused and fp32_pairs "
+                    "in {-1,0,1}");
     h->tun = *t;
     return VB_OK;
 }

@@ -38,6 +38,10 @@ struct StageParams {
     int force_box;       // 1: use the box-tile kernel even where the z-marching one fits
     int split;           // 1: z-marching stencil kernel writes U only; k_c2p solves con2prim
     int skip_c2p;        // 1: the stencil kernel writes U only and launches no con2prim
+    int pairs;           // 1: FP32-bulk 3D stages use the z-pair kernel where it exists
+    int div_in_pout;     // 1: the stencil kernel left the FP32 divergence in Pout; the
+                         //    con2prim kernel forms Uo = rk_a U0 + rk_b (Us - div) itself
+    int want_div;        // 1: the caller's con2prim kernel (skip_c2p) accepts div_in_pout
 };
 
 template <typename R> struct StageBufs {
@@ -90,6 +94,14 @@ cudaError_t launch_ref1d_store(const Ref1DState& st, double* P_aos, cudaStream_t
 
 int max_speed_blocks(const Grid& g);
 
+// FP32-bulk z-pair variant of the 3D stage (vb_stage_zp.cuh, instantiated in
+// vb_stage_f32.cu): WENOZ reconstruction with HLL or HLLC
+inline bool zp_available(int rec, int rs) { return rec == 2 && (rs == 0 || rs == 1); }
+cudaError_t launch_stage_zp(int rs, const StageParams& p, const StageBufs<float>& b, cudaStream_t s);
+// 1 when launch_stage with these arguments leaves the FP32 divergence in Pout
+// for the caller's con2prim kernel (z-pair kernel with skip_c2p and want_div)
+template <typename R> int stage_div_in_pout(int dims, int rec, int rs, const StageParams& p);
+
 // split con2prim of a 3D stage on its own (vb_stage_zm.cuh)
 template <typename R> cudaError_t launch_c2p(const StageParams& p, const StageBufs<R>& b, cudaStream_t s);
 
@@ -100,8 +112,8 @@ cudaError_t launch_mlp_guess(const void* mlp_blob, const StageParams& p, const d
 // the same guess and the W Newton from it in one kernel (vb_mlp.cu): U of the
 // stage in, the floored P of every interior cell out
 template <typename R>
-cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const double* U, R* Pout,
-                               unsigned int* err, cudaStream_t s);
+cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const StageBufs<R>& b, unsigned int* err,
+                               cudaStream_t s);
 
 // point kernels (FP64, vb_stage_f64.cu)
 cudaError_t launch_point_recon(int method, const double* q, double* out, int n, cudaStream_t s);

@@ -797,11 +797,13 @@ cudaError_t launch_mlp_guess(const void* mlp_blob, const StageParams& p, const d
 // from it (no W guess array in HBM), and the Newton's FP64 work of the other
 // CTAs on the SM overlaps each CTA's MMA round trips. W0 is rounded to FP32
 // exactly as the two-kernel form stores it, so both forms start the Newton
-// from the same guess.
+// from the same guess. With p.div_in_pout the stencil kernel left the FP32
+// divergence in Pout, and this kernel forms U = rk_a U0 + rk_b (Us - div)
+// (written to Uo) before the features; the next tile's inputs are loaded
+// before the current tile's Newton, whose latency covers them.
 template <typename R>
 __global__ void __launch_bounds__(TILE, 4) k_c2p_learned(const MlpBlob* __restrict__ blob, StageParams p,
-                                                         const double* __restrict__ U, R* __restrict__ Pout,
-                                                         unsigned int* err) {
+                                                         StageBufs<R> b, unsigned int* err) {
     extern __shared__ __align__(128) unsigned char smraw[];
     InferSmem& s = *reinterpret_cast<InferSmem*>(smraw);
     const int t = threadIdx.x;
@@ -818,27 +820,54 @@ __global__ void __launch_bounds__(TILE, 4) k_c2p_learned(const MlpBlob* __restri
         c = i + p.sy * j + p.sz * k;
         return true;
     };
+    const bool div = p.div_in_pout != 0, rk = p.rk_a != 0.0;
+    // raw inputs of one cell: U of the stage, or (Us, U0, div)
+    struct Raw {
+        double us[5], u0[5];
+        float d[5];
+    };
+    auto load = [&](long long cc, Raw& r) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            r.us[v] = div ? b.Us[v * vs + cc] : b.Uo[v * vs + cc];
+            r.u0[v] = div && rk ? b.U0[v * vs + cc] : 0.0;
+            r.d[v] = div ? (float)b.Pout[v * vs + cc] : 0.0f;
+        }
+    };
+    auto form = [&](const Raw& r, long long cc, double* uo) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            if (div) {
+                double x = r.us[v] - (double)r.d[v];
+                if (rk) x = p.rk_a * r.u0[v] + p.rk_b * x;
+                uo[v] = x;
+                b.Uo[v * vs + cc] = x;
+            } else {
+                uo[v] = r.us[v];
+            }
+        }
+    };
     unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
     uint32_t phase = 0;
     long long tile = blockIdx.x;
     long long c = 0;
     bool ok = tile < ntiles && cell(tile * TILE + t, c);
     double u[5] = {1.0, -2.0, 0.0, 0.0, 0.0};
-    if (ok)
-#pragma unroll
-        for (int v = 0; v < 5; ++v) u[v] = U[v * vs + c];
+    if (ok) {
+        Raw r;
+        load(c, r);
+        form(r, c, u);
+    }
     for (; tile < ntiles; tile += gridDim.x) {
         const long long nt = tile + gridDim.x;
         long long cn = 0;
         const bool okn = nt < ntiles && cell(nt * TILE + t, cn);
-        double un[5] = {1.0, -2.0, 0.0, 0.0, 0.0};
-        if (okn)
-#pragma unroll
-            for (int v = 0; v < 5; ++v) un[v] = U[v * vs + cn];
         float f[4];
         guess_features(u, (float)p.gamma, s.mu, s.isd, f);
         float y = 0.f;
         if (!mlp_forward_tile(s, f, y, phase, err)) break;
+        Raw rn;
+        if (okn) load(cn, rn);
         if (ok) {
             const double W0 = (double)(float)(-u[1] * (1.0 + (double)fmaxf(y, 0.0f)));
             double P[5];
@@ -851,12 +880,11 @@ __global__ void __launch_bounds__(TILE, 4) k_c2p_learned(const MlpBlob* __restri
             P[0] = jmax(P[0], p.floor_);
             P[1] = jmax(P[1], p.floor_);
 #pragma unroll
-            for (int v = 0; v < 5; ++v) Pout[v * vs + c] = (R)P[v];
+            for (int v = 0; v < 5; ++v) b.Pout[v * vs + c] = (R)P[v];
         }
+        if (okn) form(rn, cn, u);
         ok = okn;
         c = cn;
-#pragma unroll
-        for (int v = 0; v < 5; ++v) u[v] = un[v];
     }
     infer_end(s);
     unsigned long long* cnt = p.counters;
@@ -879,8 +907,8 @@ __global__ void __launch_bounds__(TILE, 4) k_c2p_learned(const MlpBlob* __restri
 }
 
 template <typename R>
-cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const double* U, R* Pout,
-                               unsigned int* err, cudaStream_t s) {
+cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const StageBufs<R>& b, unsigned int* err,
+                               cudaStream_t s) {
     static unsigned long long attr = 0;
     static int resident[64] = {0};
     int dev = 0;
@@ -905,12 +933,12 @@ cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const
     const long long tiles = (cells + TILE - 1) / TILE;
     const int nb = (int)std::min<long long>(tiles, resident[d]);
     if (nb <= 0) return cudaSuccess;
-    k_c2p_learned<R><<<nb, TILE, sizeof(InferSmem), s>>>((const MlpBlob*)mlp_blob, p, U, Pout, err);
+    k_c2p_learned<R><<<nb, TILE, sizeof(InferSmem), s>>>((const MlpBlob*)mlp_blob, p, b, err);
     return cudaGetLastError();
 }
-template cudaError_t launch_c2p_learned<float>(const void*, const StageParams&, const double*, float*,
+template cudaError_t launch_c2p_learned<float>(const void*, const StageParams&, const StageBufs<float>&,
                                                unsigned int*, cudaStream_t);
-template cudaError_t launch_c2p_learned<double>(const void*, const StageParams&, const double*, double*,
+template cudaError_t launch_c2p_learned<double>(const void*, const StageParams&, const StageBufs<double>&,
                                                 unsigned int*, cudaStream_t);
 }  // namespace vb
 

@@ -580,6 +580,7 @@ cudaError_t launch_max_speed(const Grid& g, const R* P, double gamma, double* pa
     template cudaError_t launch_bc_face<R>(const Grid&, R*, int, int, const double*, cudaStream_t);  \
     template cudaError_t launch_bc_decay<R>(const Grid&, R*, int, int, double, cudaStream_t);        \
     template cudaError_t launch_max_speed<R>(const Grid&, const R*, double, double*, int, double*,   \
-                                             cudaStream_t);
+                                             cudaStream_t);                                          \
+    template int stage_div_in_pout<R>(int, int, int, const StageParams&);
 
 }  // namespace vb

@@ -19,6 +19,8 @@
 // (x, y, z), then the RK combination, con2prim (guess = this stage's P) and
 // the floors, as in k_stage.
 #pragma once
+#include <type_traits>
+
 #include "vb_stage.cuh"
 
 namespace vb {
@@ -421,8 +423,16 @@ cudaError_t launch_stage_zm(const StageParams& p, const StageBufs<R>& b, cudaStr
                                    : launch_stage_zm_t<REC, RS, R, false>(p, b, s);
 }
 
+template <typename R> int stage_div_in_pout(int dims, int rec, int rs, const StageParams& p) {
+    if (!std::is_same<R, float>::value || dims != 3 || p.force_box || !zm_fits<R>(p)) return 0;
+    return p.pairs && zp_available(rec, rs) && p.skip_c2p && p.want_div ? 1 : 0;
+}
+
 template <typename R>
 cudaError_t dispatch_stage_zm(int rec, int rs, const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
+    if constexpr (std::is_same<R, float>::value) {
+        if (p.pairs && zp_available(rec, rs)) return launch_stage_zp(rs, p, b, s);
+    }
 #define VB_CASE(RC, RSC) \
     if (rec == RC && rs == RSC) return launch_stage_zm<RC, RSC, R>(p, b, s);
     VB_CASE(REC_MINMOD, RS_HLL)

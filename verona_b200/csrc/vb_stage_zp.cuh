@@ -1,0 +1,602 @@
+// Z-pair 3D stage kernel of the FP32-bulk form: the z-marching kernel of
+// vb_stage_zm.cuh with every thread owning TWO consecutive cells (k, k+1) of
+// its (x, y) column, carried as one float2 through the whole stencil.
+//
+// sm_100a executes FP32 add / multiply / fma on register pairs
+// (FADD2 / FMUL2 / FFMA2: __fadd2_rn, __fmul2_rn, __ffma2_rn), so one
+// instruction advances both cells. Reconstruction (WENOZ), the face floors,
+// the Riemann flux (HLL / HLLC), the flux difference and its accumulation are
+// written on float2 lanes; reciprocal, square root, min/max and selects stay
+// per lane. Each barrier of the plane loop now serves two planes.
+//
+// Arithmetic differs from the scalar FP32 kernel only in rounding (packed
+// fma contraction written out by hand, 1/6 folded into the WENOZ stencil
+// weights, C^2 formed without the square root and re-square, approximate
+// reciprocal / square root); the conserved update U - div and con2prim stay
+// FP64 exactly as in k_stage_zm. Same scheme as the reference's 3D kernels
+// (src/3dim/algos.jl:14-200, src/fluxlimiter.jl:19-71) plus HLLC.
+#pragma once
+#include "vb_stage_zm.cuh"
+
+namespace vb {
+namespace pk {
+
+using f2 = float2;
+__device__ __forceinline__ f2 P2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ f2 S2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ f2 add(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 mul(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+// a - b, exact in the product: b * (-1) + a
+__device__ __forceinline__ f2 sub(f2 a, f2 b) { return __ffma2_rn(b, S2(-1.0f), a); }
+__device__ __forceinline__ float rcp1(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sqrt1(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+// NaN-propagating max / min (Julia's Base.max / Base.min on floats)
+__device__ __forceinline__ float maxn(float a, float b) {
+    float r;
+    asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float minn(float a, float b) {
+    float r;
+    asm("min.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ f2 rcp(f2 a) { return P2(rcp1(a.x), rcp1(a.y)); }
+__device__ __forceinline__ f2 vsqrt(f2 a) { return P2(sqrt1(a.x), sqrt1(a.y)); }
+__device__ __forceinline__ f2 vmax(f2 a, f2 b) { return P2(maxn(a.x, b.x), maxn(a.y, b.y)); }
+__device__ __forceinline__ f2 vmin(f2 a, f2 b) { return P2(minn(a.x, b.x), minn(a.y, b.y)); }
+__device__ __forceinline__ f2 vabs(f2 a) { return P2(fabsf(a.x), fabsf(a.y)); }
+struct m2 {
+    bool x, y;
+};
+// 4-byte global -> shared copy that bypasses the registers (completes asynchronously)
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(sdst)),
+                 "l"(gsrc)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ f2 sel(m2 m, f2 a, f2 b) { return P2(m.x ? a.x : b.x, m.y ? a.y : b.y); }
+
+// WENOZ (src/fluxlimiter.jl:19-71) on two cells: returns (qr_i, ql_ip1).
+// FP32 epsilon 1e-30 and the 1e15 cap of the smoothness ratio as the scalar
+// FP32 form; the factor 1/(6 sum alpha) is applied as 1/6 in the stencil
+// weights and one reciprocal of sum alpha.
+__device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& qr, f2& ql) {
+    const f2 c1 = S2(13.0f / 12.0f), c2 = S2(0.25f);
+    f2 t = fma(S2(-2.0f), qm1, add(qm2, q0));
+    f2 u = fma(S2(-4.0f), qm1, fma(S2(3.0f), q0, qm2));
+    const f2 b1 = fma(mul(c1, t), t, mul(mul(c2, u), u));
+    t = fma(S2(-2.0f), q0, add(qm1, qp1));
+    u = sub(qm1, qp1);
+    const f2 b2 = fma(mul(c1, t), t, mul(mul(c2, u), u));
+    t = fma(S2(-2.0f), qp1, add(qp2, q0));
+    u = fma(S2(-4.0f), qp1, fma(S2(3.0f), q0, qp2));
+    const f2 b3 = fma(mul(c1, t), t, mul(mul(c2, u), u));
+    const f2 eps = S2(1.0e-30f);
+    const f2 tau = vabs(sub(b1, b3));
+    f2 i1 = mul(tau, rcp(add(b1, eps)));
+    f2 i2 = mul(tau, rcp(add(b2, eps)));
+    f2 i3 = mul(tau, rcp(add(b3, eps)));
+    i1 = P2(fminf(i1.x, 1.0e15f), fminf(i1.y, 1.0e15f));
+    i2 = P2(fminf(i2.x, 1.0e15f), fminf(i2.y, 1.0e15f));
+    i3 = P2(fminf(i3.x, 1.0e15f), fminf(i3.y, 1.0e15f));
+    const f2 one = S2(1.0f);
+    const f2 s1 = fma(i1, i1, one), s2 = fma(i2, i2, one), s3 = fma(i3, i3, one);
+    const f2 a2 = mul(S2(0.6f), s2);
+    // right face of cell i (left-biased stencils)
+    {
+        const f2 a1 = mul(S2(0.1f), s1), a3 = mul(S2(0.3f), s3);
+        const f2 f1 = fma(S2(11.0f / 6.0f), q0, fma(S2(-7.0f / 6.0f), qm1, mul(S2(2.0f / 6.0f), qm2)));
+        const f2 f2_ = fma(S2(2.0f / 6.0f), qp1, fma(S2(5.0f / 6.0f), q0, mul(S2(-1.0f / 6.0f), qm1)));
+        const f2 f3 = fma(S2(-1.0f / 6.0f), qp2, fma(S2(5.0f / 6.0f), qp1, mul(S2(2.0f / 6.0f), q0)));
+        ql = mul(fma(f3, a3, fma(f2_, a2, mul(f1, a1))), rcp(add(add(a1, a2), a3)));
+    }
+    // left face of cell i (right-biased stencils)
+    {
+        const f2 a1 = mul(S2(0.1f), s3), a3 = mul(S2(0.3f), s1);
+        const f2 f1 = fma(S2(11.0f / 6.0f), q0, fma(S2(-7.0f / 6.0f), qp1, mul(S2(2.0f / 6.0f), qp2)));
+        const f2 f2_ = fma(S2(2.0f / 6.0f), qm1, fma(S2(5.0f / 6.0f), q0, mul(S2(-1.0f / 6.0f), qp1)));
+        const f2 f3 = fma(S2(-1.0f / 6.0f), qm2, fma(S2(5.0f / 6.0f), qm1, mul(S2(2.0f / 6.0f), q0)));
+        qr = mul(fma(f3, a3, fma(f2_, a2, mul(f1, a1))), rcp(add(add(a1, a2), a3)));
+    }
+}
+
+// One face state along axis D (compile time): the primitive state and what
+// the HARM speeds / HLL / HLLC need from it (src/3dim/algos.jl:117-157).
+// Sign convention of the energy slot: E = -U[1] > 0 and FE = -F[1].
+template <int D> struct Side {
+    f2 P[5];
+    f2 gam, gw, uw, vn, p, lp, lm;
+    __device__ __forceinline__ void make(f2 g, f2 gm1, const f2* Pin) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) P[v] = Pin[v];
+        const f2 one = S2(1.0f);
+        gam = vsqrt(fma(P[4], P[4], fma(P[3], P[3], fma(P[2], P[2], one))));
+        const f2 w = fma(g, P[1], P[0]);
+        const f2 un = P[2 + D];
+        gw = mul(gam, w);
+        uw = mul(un, w);
+        const f2 igam = rcp(gam);
+        vn = mul(un, igam);
+        p = mul(gm1, P[1]);
+        // C^2 = Gamma (Gamma - 1) u / (rho + Gamma u) = Gamma p / w  (SoundSpeed, src/eos.jl:15-21)
+        const f2 C2 = mul(mul(g, p), rcp(w));
+        const f2 sig = mul(C2, mul(mul(igam, igam), rcp(sub(one, C2))));
+        const f2 r = vsqrt(mul(sig, add(sub(one, mul(vn, vn)), sig)));
+        const f2 inv = rcp(add(one, sig));
+        lp = mul(add(vn, r), inv);
+        lm = mul(sub(vn, r), inv);
+    }
+    // conserved component v in the energy-positive convention (slot 1 = E)
+    __device__ __forceinline__ f2 U(int v) const {
+        if (v == 0) return mul(gam, P[0]);
+        if (v == 1) return fma(gam, gw, mul(S2(-1.0f), p));
+        return mul(P[v], gw);
+    }
+    // flux component v along D, energy slot = FE
+    __device__ __forceinline__ f2 F(int v) const {
+        if (v == 0) return mul(P[0], P[2 + D]);
+        if (v == 1) return mul(uw, gam);
+        if (v == 2 + D) return fma(P[2 + D], uw, p);
+        return mul(P[v], uw);
+    }
+};
+
+// HLL (RS_HLL, src/3dim/algos.jl:149-174) or HLLC (RS_HLLC: Mignone & Bodo
+// 2005 with the HLL fallback for an unphysical star state) flux of two faces.
+template <int D, int RS>
+__device__ __forceinline__ void face_flux(f2 g, f2 gm1, const f2* PL, const f2* PR, f2* Fo) {
+    Side<D> L, R;
+    L.make(g, gm1, PL);
+    R.make(g, gm1, PR);
+    const f2 lR = vmax(L.lp, R.lp);  // Cmax
+    const f2 lL = vmin(L.lm, R.lm);  // -Cmin
+    const f2 idl = rcp(sub(lR, lL));
+    const f2 lRL = mul(lR, lL);
+    const m2 use_R{lR.x < 0.0f, lR.y < 0.0f};
+    const m2 use_L{!use_R.x && lL.x > 0.0f, !use_R.y && lL.y > 0.0f};
+    // HLL flux, energy-positive convention
+    f2 Fh[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+        Fh[v] = mul(fma(lRL, sub(R.U(v), L.U(v)), fma(lR, L.F(v), mul(mul(S2(-1.0f), lL), R.F(v)))), idl);
+    if (RS == RS_HLL) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            f2 o = sel(use_R, R.F(v), sel(use_L, L.F(v), Fh[v]));
+            Fo[v] = v == 1 ? mul(S2(-1.0f), o) : o;
+        }
+        return;
+    }
+    // star state: E_h, m_h are the HLL state, FE_h, Fm_h the HLL flux
+    const f2 E_h = mul(sub(sub(mul(lR, R.U(1)), mul(lL, L.U(1))), sub(R.F(1), L.F(1))), idl);
+    const f2 m_h = mul(sub(sub(mul(lR, R.U(2 + D)), mul(lL, L.U(2 + D))), sub(R.F(2 + D), L.F(2 + D))), idl);
+    const f2 FE_h = Fh[1], Fm_h = Fh[2 + D];
+    const f2 b = add(E_h, Fm_h);
+    f2 disc = fma(S2(-4.0f), mul(FE_h, m_h), mul(b, b));
+    disc = P2(disc.x < 0.0f ? 0.0f : disc.x, disc.y < 0.0f ? 0.0f : disc.y);
+    const f2 ls = mul(mul(S2(2.0f), m_h), rcp(add(b, vsqrt(disc))));
+    const f2 ps = fma(S2(-1.0f), mul(FE_h, ls), Fm_h);
+    const m2 left{ls.x >= 0.0f, ls.y >= 0.0f};
+    // side K behind the contact
+    const f2 lK = sel(left, lL, lR);
+    const f2 vn = sel(left, L.vn, R.vn);
+    const f2 p = sel(left, L.p, R.p);
+    const f2 ilk = rcp(sub(lK, ls));
+    const f2 dv = sub(lK, vn);
+    const f2 fac = mul(dv, ilk);
+    const m2 use_hll{!use_R.x && !use_L.x && (!(ps.x > 0.0f) || !(ls.x >= lL.x && ls.x <= lR.x)),
+                     !use_R.y && !use_L.y && (!(ps.y > 0.0f) || !(ls.y >= lL.y && ls.y <= lR.y))};
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        const f2 UK = sel(left, L.U(v), R.U(v));
+        const f2 FK = sel(left, L.F(v), R.F(v));
+        f2 Us;
+        if (v == 1)  // E* = (E (lK - vn) + p* ls - p vn) / (lK - ls)
+            Us = mul(fma(UK, dv, sub(mul(ps, ls), mul(p, vn))), ilk);
+        else if (v == 2 + D)  // m* = (m (lK - vn) + p* - p) / (lK - ls)
+            Us = mul(add(fma(UK, dv, ps), mul(S2(-1.0f), p)), ilk);
+        else
+            Us = mul(UK, fac);
+        const f2 fs = fma(lK, sub(Us, UK), FK);
+        f2 o = sel(use_R, R.F(v), sel(use_L, L.F(v), sel(use_hll, Fh[v], fs)));
+        Fo[v] = v == 1 ? mul(S2(-1.0f), o) : o;
+    }
+}
+
+}  // namespace pk
+
+template <int TX, int TY> struct ZpGeom {
+    static constexpr int NV = 5, NT = TX * TY;
+    static constexpr int EX = TX + 6, EY = TY + 6;
+    static constexpr int PLN = EX * EY;
+    static constexpr int FXN = (TX + 1) * TY, FYN = TX * (TY + 1);
+    static constexpr int FN = FXN > FYN ? FXN : FYN;
+    static constexpr int QXN = TX > TY ? TX : TY;
+    static constexpr int ZR = 6;  // z-window ring: planes k-1 .. k+4
+    static constexpr size_t smem_bytes() {
+        return sizeof(float2) * NV * (size_t)(PLN + 2 * FN + QXN) + sizeof(float) * (size_t)ZR * NV * NT;
+    }
+};
+
+// What a pair stage kernel leaves behind: con2prim done in the kernel (fused),
+// U for k_c2p (split), or the FP32 divergence in Pout for the learned
+// con2prim kernel, which forms U itself (div).
+enum { ZP_FUSED = 0, ZP_U = 1, ZP_DIV = 2 };
+
+template <int RS, int TX, int TY, int LZ, int MINB, int TAIL>
+__global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, StageBufs<float> b) {
+    using namespace pk;
+    using G = ZpGeom<TX, TY>;
+    constexpr int NV = 5, NT = G::NT, EX = G::EX, PLN = G::PLN, FN = G::FN, QXN = G::QXN, ZR = G::ZR;
+    constexpr int FXR = TX + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    f2* sPl = reinterpret_cast<f2*>(smem_raw);  // [NV][EY][EX]: planes (k, k+1) with x/y halo
+    f2* sQL = sPl + NV * PLN;                     // [NV][FN]: left states of the faces
+    f2* sF = sQL + NV * FN;                       // [NV][FN]: face fluxes
+    f2* sQX = sF + NV * FN;                       // [NV][QXN]: right states of the last faces
+    float* sZ = reinterpret_cast<float*>(sQX + NV * QXN);  // [ZR][NV][NT]: this thread's z-window
+
+    const int tid = threadIdx.x;
+    const int tx = tid % TX, ty = tid / TX;
+    const int i0 = NG + blockIdx.x * TX, j0 = NG + blockIdx.y * TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const int z0 = NG + blockIdx.z * LZ;
+    const int zend = min(z0 + LZ, p.n[2] - NG);
+    const long long sy = p.sy, sz = p.sz, vs = p.vs;
+    const long long col = i + sy * j;
+    const f2 fl = S2((float)p.floor_);
+    const f2 g = S2((float)p.gamma), gm1 = S2((float)(p.gamma - 1.0));
+    const f2 cx = S2((float)p.dtdx[0]), cy = S2((float)p.dtdx[1]), cz = S2((float)p.dtdx[2]);
+
+    auto zs = [&](int z, int v) -> float& { return sZ[((z % ZR) * NV + v) * NT + tid]; };
+    auto zload = [&](int z) {
+        const bool in = z < p.n[2];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) zs(z, v) = in ? b.Pin[v * vs + col + sz * z] : 0.0f;
+    };
+    // reconstruct the cells (c, c+1) along z from the window planes c-2 .. c+3, floored
+    auto zrecon = [&](int c, f2* qr, f2* ql) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const float s0 = zs(c - 2, v), s1 = zs(c - 1, v), s2 = zs(c, v), s3 = zs(c + 1, v), s4 = zs(c + 2, v),
+                        s5 = zs(c + 3, v);
+            wenoz(P2(s0, s1), P2(s1, s2), P2(s2, s3), P2(s3, s4), P2(s4, s5), qr[v], ql[v]);
+            if (v < 2) {
+                qr[v] = vmax(fl, qr[v]);
+                ql[v] = vmax(fl, ql[v]);
+            }
+        }
+    };
+
+    // x/y halo of the planes (kk, kk+1) -> sPl, by asynchronous copies: issued for
+    // the next pair once the current pair's x/y reconstructions are done, and
+    // waited for at the next pair's first barrier
+    constexpr int NXH = 6 * TY, NH = NXH + 6 * TX;
+    auto halo_issue = [&](int kk) {
+        for (int e = tid; e < NH; e += NT) {
+            int hx, hy;
+            if (e < NXH) {
+                int s6 = e % 6;
+                hy = e / 6;
+                hx = s6 < 3 ? s6 - 3 : TX + s6 - 3;
+            } else {
+                int e2 = e - NXH, s6 = e2 / TX;
+                hx = e2 % TX;
+                hy = s6 < 3 ? s6 - 3 : TY + s6 - 3;
+            }
+            const long long gc = (i0 + hx) + sy * (j0 + hy) + sz * kk;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                f2* d = &sPl[v * PLN + (hy + 3) * EX + hx + 3];
+                cp_async4(&d->x, b.Pin + v * vs + gc);
+                cp_async4(&d->y, b.Pin + v * vs + gc + sz);
+            }
+        }
+    };
+    halo_issue(z0);
+
+    float qlz[NV];  // ql of cell k (left state of face k+1/2)
+    float Fzm[NV];  // flux at face k-1/2
+    // prologue: window z0-3 .. z0+2, cells (z0-1, z0), the flux at z0-1/2 (both lanes), then z0+3, z0+4
+    for (int z = z0 - 3; z <= z0 + 2; ++z) zload(z);
+    {
+        f2 qr[NV], ql[NV], L[NV], R[NV], F[NV];
+        zrecon(z0 - 1, qr, ql);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            L[v] = S2(ql[v].x);
+            R[v] = S2(qr[v].y);
+            qlz[v] = ql[v].y;
+        }
+        face_flux<2, RS>(g, gm1, L, R, F);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Fzm[v] = F[v].x;
+    }
+    zload(z0 + 3);
+    zload(z0 + 4);
+
+    unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
+    for (int k = z0; k < zend; k += 2) {
+        const bool two = k + 1 < zend;
+        const long long c = col + sz * k;
+        f2 acc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[v] = S2(0.0f);
+
+        // stage planes (k, k+1): own column from the window; the halo copies were
+        // issued earlier (plane k+1 <= zend <= n2 - 3 exists even when the pair is incomplete)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) sPl[v * PLN + (ty + 3) * EX + tx + 3] = P2(zs(k, v), zs(k + 1, v));
+        cp_async_wait_all();
+        __syncthreads();
+
+        // x: reconstruct own cells; halo cells -1 and TX of each row
+        f2 qrx[NV];
+        {
+            const f2* q = sPl + (ty + 3) * EX + tx + 3;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const f2* qv = q + v * PLN;
+                f2 qr, ql;
+                wenoz(qv[-2], qv[-1], qv[0], qv[1], qv[2], qr, ql);
+                if (v < 2) {
+                    qr = vmax(fl, qr);
+                    ql = vmax(fl, ql);
+                }
+                qrx[v] = qr;
+                sQL[v * FN + ty * FXR + tx + 1] = ql;
+            }
+        }
+        for (int e = NT - 1 - tid; e >= 0 && e < 2 * TY; e += NT) {
+            const int r = e >> 1, side = e & 1;
+            const f2* q = sPl + (r + 3) * EX + (side ? TX : -1) + 3;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const f2* qv = q + v * PLN;
+                f2 qr, ql;
+                wenoz(qv[-2], qv[-1], qv[0], qv[1], qv[2], qr, ql);
+                if (v < 2) {
+                    qr = vmax(fl, qr);
+                    ql = vmax(fl, ql);
+                }
+                if (side)
+                    sQX[v * QXN + r] = qr;
+                else
+                    sQL[v * FN + r * FXR] = ql;
+            }
+        }
+        __syncthreads();
+        {
+            f2 PL[NV], F[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) PL[v] = sQL[v * FN + ty * FXR + tx];
+            face_flux<0, RS>(g, gm1, PL, qrx, F);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) sF[v * FN + ty * FXR + tx] = F[v];
+        }
+        for (int e = NT - 1 - tid; e >= 0 && e < TY; e += NT) {
+            f2 PL[NV], PR[NV], F[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                PL[v] = sQL[v * FN + e * FXR + TX];
+                PR[v] = sQX[v * QXN + e];
+            }
+            face_flux<0, RS>(g, gm1, PL, PR, F);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) sF[v * FN + e * FXR + TX] = F[v];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+            acc[v] = fma(cx, sub(sF[v * FN + ty * FXR + tx + 1], sF[v * FN + ty * FXR + tx]), acc[v]);
+
+        // y: reconstruct own cells; halo cells -1 and TY of each column
+        f2 qry[NV];
+        {
+            const f2* q = sPl + (ty + 3) * EX + tx + 3;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const f2* qv = q + v * PLN;
+                f2 qr, ql;
+                wenoz(qv[-2 * EX], qv[-EX], qv[0], qv[EX], qv[2 * EX], qr, ql);
+                if (v < 2) {
+                    qr = vmax(fl, qr);
+                    ql = vmax(fl, ql);
+                }
+                qry[v] = qr;
+                sQL[v * FN + (ty + 1) * TX + tx] = ql;
+            }
+        }
+        for (int e = tid; e < 2 * TX; e += NT) {
+            const int cx_ = e % TX, side = e / TX;
+            const f2* q = sPl + ((side ? TY : -1) + 3) * EX + cx_ + 3;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const f2* qv = q + v * PLN;
+                f2 qr, ql;
+                wenoz(qv[-2 * EX], qv[-EX], qv[0], qv[EX], qv[2 * EX], qr, ql);
+                if (v < 2) {
+                    qr = vmax(fl, qr);
+                    ql = vmax(fl, ql);
+                }
+                if (side)
+                    sQX[v * QXN + cx_] = qr;
+                else
+                    sQL[v * FN + cx_] = ql;
+            }
+        }
+        __syncthreads();
+        // every read of sPl for this pair is done: fetch the next pair's halo
+        if (k + 2 < zend) halo_issue(k + 2);
+        {
+            f2 PL[NV], F[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) PL[v] = sQL[v * FN + ty * TX + tx];
+            face_flux<1, RS>(g, gm1, PL, qry, F);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) sF[v * FN + ty * TX + tx] = F[v];
+        }
+        for (int e = NT - 1 - tid; e >= 0 && e < TX; e += NT) {
+            f2 PL[NV], PR[NV], F[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                PL[v] = sQL[v * FN + TY * TX + e];
+                PR[v] = sQX[v * QXN + e];
+            }
+            face_flux<1, RS>(g, gm1, PL, PR, F);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) sF[v * FN + TY * TX + e] = F[v];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+            acc[v] = fma(cy, sub(sF[v * FN + (ty + 1) * TX + tx], sF[v * FN + ty * TX + tx]), acc[v]);
+
+        // z: planes k+5, k+6 are fetched now and enter the window after the
+        // reconstruction of cells (k+1, k+2) from planes k-1 .. k+4; faces
+        // k+1/2 (left ql(k), right qr(k+1)) and k+3/2 (left ql(k+1), right qr(k+2))
+        float nxt[2 * NV];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const bool in = k + 5 + q < p.n[2];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) nxt[q * NV + v] = in ? b.Pin[v * vs + c + (5 + q) * sz] : 0.0f;
+        }
+        float Pk[2 * NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            Pk[v] = zs(k, v);
+            Pk[NV + v] = zs(k + 1, v);
+        }
+        {
+            f2 qr1[NV], ql1[NV], L[NV], Fz[NV];
+            zrecon(k + 1, qr1, ql1);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) L[v] = P2(qlz[v], ql1[v].x);
+            face_flux<2, RS>(g, gm1, L, qr1, Fz);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                acc[v] = fma(cz, sub(Fz[v], P2(Fzm[v], Fz[v].x)), acc[v]);
+                Fzm[v] = Fz[v].y;
+                qlz[v] = ql1[v].y;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) zs(k + 5 + q, v) = nxt[q * NV + v];
+
+        // ZP_DIV: the FP32 divergence into Pout; ZP_U: the RK combination in FP64
+        // (U - div) into Uo; ZP_FUSED: that, then con2prim (guess: this stage's P)
+        // and the floors
+        if (TAIL == ZP_DIV) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                b.Pout[v * vs + c] = acc[v].x;
+                if (two) b.Pout[v * vs + c + sz] = acc[v].y;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < (TAIL == ZP_DIV ? 0 : 2); ++q) {
+            if (q == 1 && !two) break;
+            const long long cc = c + q * sz;
+            double U[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                double u = b.Us[v * vs + cc] - (double)(q ? acc[v].y : acc[v].x);
+                if (p.rk_a != 0.0) u = p.rk_a * b.U0[v * vs + cc] + p.rk_b * u;
+                U[v] = u;
+                b.Uo[v * vs + cc] = u;
+            }
+            if (TAIL == ZP_FUSED) {
+                double P[NV];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) P[v] = (double)Pk[q * NV + v];
+                int fb;
+                int r = solve_cell<3>(p, U, P, cc, fb);
+                n_fail += (r < 0);
+                n_fb += fb;
+                n_it += (r < 0 ? -r : r);
+                n_cells += 1;
+                P[0] = jmax(P[0], p.floor_);
+                P[1] = jmax(P[1], p.floor_);
+#pragma unroll
+                for (int v = 0; v < NV; ++v) b.Pout[v * vs + cc] = (float)P[v];
+            }
+        }
+    }
+
+    if (n_fail) count_add(p.counters, CNT_C2P_FAIL, n_fail);
+    if (p.stats) {
+        for (int o = 16; o > 0; o >>= 1) {
+            n_fb += __shfl_xor_sync(0xffffffffu, n_fb, o);
+            n_it += __shfl_xor_sync(0xffffffffu, n_it, o);
+            n_cells += __shfl_xor_sync(0xffffffffu, n_cells, o);
+        }
+        if ((tid & 31) == 0) {
+            count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
+            count_add(p.counters, CNT_C2P_ITERS, n_it);
+            count_add(p.counters, CNT_C2P_CELLS, n_cells);
+        }
+    } else if (n_fb) {
+        count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
+    }
+}
+
+// Tile shape of the z-pair kernel: same column tile as the scalar FP32
+// z-marching kernel; 2 CTAs of 256 threads per SM (128 registers each).
+struct ZpCfg {
+    static constexpr int TX = 32, TY = 8, LZ = 64, MINB = 2, MINB_SPLIT = 2;
+};
+
+template <int RS, int TAIL>
+cudaError_t launch_stage_zp_t(const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
+    using C = ZpCfg;
+    using G = ZpGeom<C::TX, C::TY>;
+    auto kern = k_stage_zp<RS, C::TX, C::TY, C::LZ, TAIL == ZP_FUSED ? C::MINB : C::MINB_SPLIT, TAIL>;
+    constexpr size_t smem = G::smem_bytes();
+    static unsigned long long attr_set = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(attr_set >> (dev & 63) & 1ULL)) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
+        attr_set |= 1ULL << (dev & 63);
+    }
+    dim3 grid((p.n[0] - 2 * NG) / C::TX, (p.n[1] - 2 * NG) / C::TY, (p.n[2] - 2 * NG + C::LZ - 1) / C::LZ);
+    kern<<<grid, C::TX * C::TY, smem, s>>>(p, b);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || TAIL != ZP_U || p.skip_c2p) return e;
+    const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
+    k_c2p<float><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
+    return cudaGetLastError();
+}
+
+// WENOZ with HLL or HLLC in the FP32-bulk form (zp_available). The divergence
+// hand-off (ZP_DIV) is taken when the caller's con2prim kernel forms U itself
+// (p.want_div, the fused learned kernel), which saves the stencil kernel every
+// FP64 load and store; the reference con2prim cascade of k_c2p, bound by its
+// own memory latency, keeps reading a formed U (ZP_U).
+template <int RS> cudaError_t dispatch_stage_zp_rs(const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
+    if (!(p.split || p.skip_c2p)) return launch_stage_zp_t<RS, ZP_FUSED>(p, b, s);
+    if (p.skip_c2p && p.want_div) return launch_stage_zp_t<RS, ZP_DIV>(p, b, s);
+    return launch_stage_zp_t<RS, ZP_U>(p, b, s);
+}
+inline cudaError_t dispatch_stage_zp(int rs, const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
+    return rs == RS_HLLC ? dispatch_stage_zp_rs<RS_HLLC>(p, b, s) : dispatch_stage_zp_rs<RS_HLL>(p, b, s);
+}
+
+}  // namespace vb
