@@ -433,19 +433,48 @@ static VB_NOINLINE __host__ __device__ int c2p_3d_tail(double g, int n_iter, dou
 // ---- guess-driven W Newton with a bracketed fallback -------------------------
 // Residual of the 1DW scheme (Noble et al. 2006) written in W alone:
 // f(W) = Q_t + W - k (W (1 - v^2) - D sqrt(1 - v^2)), v^2 = S^2 / W^2.
+// Evaluated from 1/W and 1/sqrt(1 - v^2), one divide and one reciprocal square
+// root per call: with a = 1 - v^2, s = sqrt(a) = a / sqrt(a),
+//   f  = Q_t + W - k (W a - D s),
+//   f' = 1 - k (a + 2 v^2 - D v^2 / (W s))       (d v^2 / dW = -2 v^2 / W),
+// k = (Gamma - 1) / Gamma.
 struct WRes {
     double f, df;
 };
-VB_HD WRes w_residual(double g, double D, double Q_t, double S2, double W) {
-    double k = (g - 1.0) / g;
-    double v2 = S2 / (W * W);
+VB_HD double rsqrt_d(double x) {
+#ifdef __CUDA_ARCH__
+    return rsqrt(x);
+#else
+    return 1.0 / sqrt(x);
+#endif
+}
+VB_HD WRes w_residual(double k, double D, double Q_t, double S2, double W) {
+    const double iW = 1.0 / W;
+    double v2 = S2 * iW * iW;
     if (v2 > 1.0 - 1e-15) v2 = 1.0 - 1e-15;
-    double s = sqrt(1.0 - v2);
+    const double a = 1.0 - v2;
+    const double rs = rsqrt_d(a);
     WRes r;
-    r.f = Q_t + W - k * (W * (1.0 - v2) - D * s);
-    double W3 = W * W * W;
-    r.df = 1.0 - k * (1.0 - v2) - k * (W * (2.0 * S2 / W3) - D * (S2 / (W3 * s)));
+    r.f = Q_t + W - k * (W * a - D * (a * rs));
+    r.df = 1.0 - k * (a + 2.0 * v2 - D * v2 * iW * rs);
     return r;
+}
+
+// The final-state formula of prims_from_W (src/3dim/structs.jl:334-340) from
+// 1/W and 1/sqrt(1 - v^2) (the W Newton's refinement, not the reference
+// cascade, whose prims_from_W keeps the reference's operation order).
+VB_HD void prims_from_W_fast(double g, double D, double Qx, double Qy, double Qz, double S2, double W, double* P) {
+    const double iW = 1.0 / W;
+    const double a = 1.0 - S2 * iW * iW;
+    const double rs = rsqrt_d(a);
+    const double gm = jmin(rs, 50.0);
+    const double igm = gm < rs ? 1.0 / 50.0 : a * rs;  // 1 / gm
+    P[0] = jmax(1e-8, D * igm);
+    P[1] = jmax(1e-8, (W * igm * igm - D * igm) / g);
+    const double f = gm * iW;
+    P[2] = Qx * f;
+    P[3] = Qy * f;
+    P[4] = Qz * f;
 }
 
 // Newton on W from a guess, to |dW| <= rtol * W, at most max_newton steps;
@@ -460,30 +489,31 @@ VB_HD int c2p_w(double g, const double* Uc, double W0, double rtol, int max_newt
     const double Qx = Uc[2], Qy = Uc[3], Qz = Uc[4];
     const double S2 = Qx * Qx + Qy * Qy + Qz * Qz;
     const double Wlo0 = sqrt(S2) * (1.0 + 1e-15);
+    const double k = (g - 1.0) / g;
     double W = W0;
     int it = 0;
     *used_fallback = 0;
     if (!(W > Wlo0) || !isfinite(W)) W = fmax(Wlo0 * 1.0000001, D - Q_t);
     for (; it < max_newton; ++it) {
-        WRes r = w_residual(g, D, Q_t, S2, W);
+        WRes r = w_residual(k, D, Q_t, S2, W);
         double dW = r.f / r.df;
         double Wn = W - dW;
         if (!(Wn > Wlo0)) Wn = 0.5 * (W + Wlo0);
         bool done = fabs(Wn - W) <= rtol * fabs(Wn);
         W = Wn;
         if (done && isfinite(W)) {
-            prims_from_W(g, D, Qx, Qy, Qz, S2, W, P);
+            prims_from_W_fast(g, D, Qx, Qy, Qz, S2, W, P);
             return it + 1;
         }
     }
     // Bracketed Newton: f(Wlo) <= 0 for a physical state; grow Whi until f > 0.
     *used_fallback = 1;
     double lo = Wlo0, hi = fmax(2.0 * Wlo0, D - Q_t + 1.0);
-    WRes rl = w_residual(g, D, Q_t, S2, lo);
-    WRes rh = w_residual(g, D, Q_t, S2, hi);
+    WRes rl = w_residual(k, D, Q_t, S2, lo);
+    WRes rh = w_residual(k, D, Q_t, S2, hi);
     for (int k = 0; k < 200 && rh.f * rl.f > 0.0; ++k) {
         hi *= 4.0;
-        rh = w_residual(g, D, Q_t, S2, hi);
+        rh = w_residual(k, D, Q_t, S2, hi);
     }
     if (!(rh.f * rl.f <= 0.0)) {
         for (int v = 0; v < 5; ++v) P[v] = vb_nan();
@@ -491,7 +521,7 @@ VB_HD int c2p_w(double g, const double* Uc, double W0, double rtol, int max_newt
     }
     W = (W > lo && W < hi) ? W : 0.5 * (lo + hi);
     for (int k = 0; k < max_bracket; ++k, ++it) {
-        WRes r = w_residual(g, D, Q_t, S2, W);
+        WRes r = w_residual(k, D, Q_t, S2, W);
         if ((r.f < 0.0) == (rl.f < 0.0)) {
             lo = W;
             rl = r;
@@ -501,7 +531,7 @@ VB_HD int c2p_w(double g, const double* Uc, double W0, double rtol, int max_newt
         double Wn = W - r.f / r.df;
         if (!(Wn > lo && Wn < hi)) Wn = 0.5 * (lo + hi);
         if (fabs(Wn - W) <= rtol * fabs(Wn) || (hi - lo) <= rtol * hi) {
-            prims_from_W(g, D, Qx, Qy, Qz, S2, Wn, P);
+            prims_from_W_fast(g, D, Qx, Qy, Qz, S2, Wn, P);
             return it + 1;
         }
         W = Wn;
