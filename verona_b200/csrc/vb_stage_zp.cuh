@@ -358,12 +358,15 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
                 sQL[v * FN + ty * FXR + tx + 1] = ql;
             }
         }
-        for (int e = NT - 1 - tid; e >= 0 && e < 2 * TY; e += NT) {
-            const int r = e >> 1, side = e & 1;
-            const f2* q = sPl + (r + 3) * EX + (side ? TX : -1) + 3;
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                const f2* qv = q + v * PLN;
+        // halo cells -1 and TX of every row, one (cell, variable) per thread and
+        // XPW per warp, so that every warp adds one reconstruction at most
+        {
+            constexpr int XH = 2 * TY * NV, NW = NT / 32, XPW = (XH + NW - 1) / NW;
+            static_assert(XPW <= 32, "x-halo items per warp");
+            const int lane = tid & 31, e = (tid >> 5) * XPW + lane;
+            if (lane < XPW && e < XH) {
+                const int v = e % NV, cell = e / NV, r = cell >> 1, side = cell & 1;
+                const f2* qv = sPl + v * PLN + (r + 3) * EX + (side ? TX : -1) + 3;
                 f2 qr, ql;
                 wenoz(qv[-2], qv[-1], qv[0], qv[1], qv[2], qr, ql);
                 if (v < 2) {
@@ -418,23 +421,20 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
                 sQL[v * FN + (ty + 1) * TX + tx] = ql;
             }
         }
-        for (int e = tid; e < 2 * TX; e += NT) {
-            const int cx_ = e % TX, side = e / TX;
-            const f2* q = sPl + ((side ? TY : -1) + 3) * EX + cx_ + 3;
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                const f2* qv = q + v * PLN;
-                f2 qr, ql;
-                wenoz(qv[-2 * EX], qv[-EX], qv[0], qv[EX], qv[2 * EX], qr, ql);
-                if (v < 2) {
-                    qr = vmax(fl, qr);
-                    ql = vmax(fl, ql);
-                }
-                if (side)
-                    sQX[v * QXN + cx_] = qr;
-                else
-                    sQL[v * FN + cx_] = ql;
+        // halo cells -1 and TY of every column, one (cell, variable) per thread
+        for (int e = tid; e < 2 * TX * NV; e += NT) {
+            const int v = e / (2 * TX), cell = e % (2 * TX), cx_ = cell % TX, side = cell / TX;
+            const f2* qv = sPl + v * PLN + ((side ? TY : -1) + 3) * EX + cx_ + 3;
+            f2 qr, ql;
+            wenoz(qv[-2 * EX], qv[-EX], qv[0], qv[EX], qv[2 * EX], qr, ql);
+            if (v < 2) {
+                qr = vmax(fl, qr);
+                ql = vmax(fl, ql);
             }
+            if (side)
+                sQX[v * QXN + cx_] = qr;
+            else
+                sQL[v * FN + cx_] = ql;
         }
         __syncthreads();
         // every read of sPl for this pair is done: fetch the next pair's halo
