@@ -206,6 +206,30 @@ def read_peaks():
         return 6650.0, "fallback"
 
 
+def fp64_gemm_tflops():
+    """FP64 denominator of the plain path's roofline: cuBLAS DGEMM 8192^3
+    through torch, best of 3 after one warm-up (B200's FP64 vector and tensor
+    rates are nominally equal)."""
+    import torch
+
+    n = 8192
+    a = torch.randn((n, n), dtype=torch.float64, device="cuda")
+    b = torch.randn((n, n), dtype=torch.float64, device="cuda")
+    c = a @ b
+    best = None
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n**3 / (best / 1e3) / 1e12
+
+
 def read_traffic(key):
     """DRAM bytes per cell of one RK-stage kernel group (the stage kernel plus
     its con2prim kernel where split) from the committed ncu summary."""
@@ -315,6 +339,16 @@ def run_ours(args, rank, world, dist):
         s.load_prims(P0)
         ms, st_ms, st_l, ln = timed_steps(s, dt, W, K, dist)
         fp64 = {"value": cells * K / (ms / 1e3), "ms_per_step": ms / K, "stage_ms_per_launch": st_ms / max(st_l, 1)}
+        # FP64 roofline of the stage group (k_stage_zm<double> + k_c2p<double>):
+        # FP64 operations per cell (2 dfma + dadd + dmul, ncu counters of one
+        # RK-stage launch pair) over the group's live time, against DGEMM
+        flop = read_traffic("fp64_previous_stage_group_flop")
+        peak64 = fp64_gemm_tflops()
+        if flop:
+            ach = flop * cells / (fp64["stage_ms_per_launch"] / 1e3) / 1e12
+            fp64["roofline"] = {"bound": "fp64", "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
+                                "frac": ach / peak64, "flop_per_cell": flop,
+                                "peak_kind": "measured in this run: cuBLAS DGEMM 8192^3 (torch)"}
         P64 = s.store_prims()
         torch.cuda.synchronize()
         info["fp64_counters"] = s.counters().tolist()
@@ -380,6 +414,7 @@ def run_ours(args, rank, world, dist):
     stage_ms_per_launch = st_ms / max(st_l, 1)
     achieved = cells * bytes_per_cell_step / 3.0 / (stage_ms_per_launch / 1e3) / 1e9
     form = "_fused" if learned_ok and args.learned_form == "fused" else ""
+    form += "_pairs" if args.stencil == "pairs" else ""
     traffic = read_traffic(f"fp32_{guess}{form}_stage_group")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
@@ -393,7 +428,9 @@ def run_ours(args, rank, world, dist):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic * cells if traffic else None, "peak_kind": peak_kind,
                      "per": "one RK-stage launch of the kernel group over the full grid",
-                     "kernel": "k_stage_zm (reconstruct+HLLC+divergence+RK) + con2prim kernel",
+                     "kernel": ("k_stage_zp (z-pair FP32 reconstruct+HLLC+divergence) + k_c2p_learned "
+                                "(RK combination, tensor-core guess, W Newton)" if learned_ok and
+                                args.learned_form == "fused" else "stencil kernel + con2prim kernel(s)"),
                      "algorithmic_bytes_per_launch": bytes_per_cell_step / 3.0 * cells,
                      "stage_ms_per_launch": stage_ms_per_launch},
         "gpu_launches": launches,
