@@ -43,6 +43,7 @@
 
 #include "../../include/verona_b200.h"
 #include "vb_con2prim.cuh"
+#include "vb_index.cuh"
 #include "vb_internal.h"
 #include "vb_tc.cuh"
 
@@ -421,13 +422,9 @@ __device__ __forceinline__ void guess_features(const double* U, float gamma, con
 }
 
 // interior cell e of the grid -> padded linear index; false past the end
-__device__ __forceinline__ bool guess_cell(const GuessArgs& a, long long e, long long tot, int N0, int N1,
-                                           long long& c) {
+__device__ __forceinline__ bool guess_cell(const CellMap& cm, long long e, long long tot, long long& c) {
     if (e >= tot) return false;
-    const int i = (int)(e % N0) + NG;
-    const int j = (int)((e / N0) % N1) + NG;
-    const int k = (int)(e / ((long long)N0 * N1)) + NG;
-    c = i + a.sy * j + a.sz * k;
+    c = cm.padded((uint32_t)e);
     return true;
 }
 
@@ -439,12 +436,14 @@ __global__ void __launch_bounds__(TILE) k_mlp_guess(const MlpBlob* __restrict__ 
     const int t = threadIdx.x;
     infer_begin(s, blob);
     const int N0 = a.n[0] - 2 * NG, N1 = a.n[1] - 2 * NG, N2 = a.n[2] - 2 * NG;
-    const long long tot = (long long)N0 * N1 * N2;
+    const long long tot = (long long)N0 * N1 * N2;  // < 2^32 (launch_mlp_guess)
     const long long ntiles = (tot + TILE - 1) / TILE;
+    CellMap cm;
+    cm.init(N0, N1, a.sy, a.sz, NG);
     uint32_t phase = 0;
     long long tile = blockIdx.x;
     long long c = 0;
-    bool ok = tile < ntiles && guess_cell(a, tile * TILE + t, tot, N0, N1, c);
+    bool ok = tile < ntiles && guess_cell(cm, tile * TILE + t, tot, c);
     double u[5] = {1.0, -2.0, 0.0, 0.0, 0.0};
     if (ok)
 #pragma unroll
@@ -452,7 +451,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_guess(const MlpBlob* __restrict__ 
     for (; tile < ntiles; tile += gridDim.x) {
         const long long nt = tile + gridDim.x;
         long long cn = 0;
-        const bool okn = nt < ntiles && guess_cell(a, nt * TILE + t, tot, N0, N1, cn);
+        const bool okn = nt < ntiles && guess_cell(cm, nt * TILE + t, tot, cn);
         double un[5] = {1.0, -2.0, 0.0, 0.0, 0.0};
         if (okn)
 #pragma unroll
@@ -811,6 +810,7 @@ cudaError_t launch_mlp_guess(const void* mlp_blob, const StageParams& p, const d
         attr |= 1ULL << (dev & 63);
     }
     const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
+    if ((unsigned long long)cells > MAX_CELLS_U32) return cudaErrorInvalidValue;
     const long long tiles = (cells + TILE - 1) / TILE;
     const int nb = (int)std::min<long long>(tiles, 148LL * 4);
     k_mlp_guess<<<nb, TILE, sizeof(InferSmem), s>>>((const MlpBlob*)mlp_blob, a);
@@ -838,12 +838,11 @@ __global__ void __launch_bounds__(TILE, 5) k_c2p_learned(const MlpBlob* __restri
     const long long tot = (long long)N0 * N1 * N2;
     const long long ntiles = (tot + TILE - 1) / TILE;
     const long long vs = p.vs;
+    CellMap cm;  // tot < 2^32 (launch_c2p_learned)
+    cm.init(N0, N1, p.sy, p.sz, NG);
     auto cell = [&](long long e, long long& c) -> bool {
         if (e >= tot) return false;
-        const int i = (int)(e % N0) + NG;
-        const int j = (int)((e / N0) % N1) + NG;
-        const int k = (int)(e / ((long long)N0 * N1)) + NG;
-        c = i + p.sy * j + p.sz * k;
+        c = cm.padded((uint32_t)e);
         return true;
     };
     const bool div = p.div_in_pout != 0, rk = p.rk_a != 0.0;
@@ -957,6 +956,7 @@ cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const
         attr |= 1ULL << d;
     }
     const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
+    if ((unsigned long long)cells > MAX_CELLS_U32) return cudaErrorInvalidValue;
     const long long tiles = (cells + TILE - 1) / TILE;
     const int nb = (int)std::min<long long>(tiles, resident[d]);
     if (nb <= 0) return cudaSuccess;

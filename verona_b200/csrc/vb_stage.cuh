@@ -14,6 +14,7 @@
 // the guess and writes U and the floored P.
 #pragma once
 #include "vb_con2prim.cuh"
+#include "vb_index.cuh"
 #include "vb_internal.h"
 
 namespace vb {

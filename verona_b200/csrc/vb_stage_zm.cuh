@@ -342,14 +342,13 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
     constexpr int NV = 5;
     const int N0 = p.n[0] - 2 * NG, N1 = p.n[1] - 2 * NG, N2 = p.n[2] - 2 * NG;
-    const long long tot = (long long)N0 * N1 * N2;
+    const long long tot = (long long)N0 * N1 * N2;  // < 2^32 (launch_c2p)
+    CellMap cm;
+    cm.init(N0, N1, p.sy, p.sz, NG);
     unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
          e += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(e % N0) + NG;
-        const int j = (int)((e / N0) % N1) + NG;
-        const int k = (int)(e / ((long long)N0 * N1)) + NG;
-        const long long c = i + p.sy * j + p.sz * k;
+        const long long c = cm.padded((uint32_t)e);
         double U[NV], P[NV];
         const bool need_p = !(p.c2p_mode == C2P_GUESS_W && p.w_guess);
 #pragma unroll
@@ -388,6 +387,7 @@ __global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
 // the split con2prim alone (3D interior), e.g. after a kernel that wrote the W guesses
 template <typename R> cudaError_t launch_c2p(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
     const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
+    if ((unsigned long long)cells > MAX_CELLS_U32) return cudaErrorInvalidValue;
     k_c2p<R><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
     return cudaGetLastError();
 }
@@ -413,6 +413,7 @@ cudaError_t launch_stage_zm_t(const StageParams& p, const StageBufs<R>& b, cudaS
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !SPLIT || p.skip_c2p) return e;
     const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
+    if ((unsigned long long)cells > MAX_CELLS_U32) return cudaErrorInvalidValue;
     k_c2p<R><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
     return cudaGetLastError();
 }
