@@ -68,20 +68,27 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 __device__ __forceinline__ f2 sel(m2 m, f2 a, f2 b) { return P2(m.x ? a.x : b.x, m.y ? a.y : b.y); }
 
 // WENOZ (src/fluxlimiter.jl:19-71) on two cells: returns (qr_i, ql_ip1).
-// FP32 epsilon 1e-30 and the 1e15 cap of the smoothness ratio as the scalar
-// FP32 form; the factor 1/(6 sum alpha) is applied as 1/6 in the stencil
-// weights and one reciprocal of sum alpha.
+// Written on the one-sided differences D1..D4 of the five values, which the
+// smoothness indicators and the three stencils share:
+//   beta_k * 12/13 = t_k^2 + (3/13) u_k^2 with the reference's t (second
+//   difference) and u (one-sided combination) of each sub-stencil;
+//   face value = q_i + sum_k d_k s_k g_k / sum_k d_k s_k, g_k = f_k - q_i,
+//   s_k = 1 + (tau5 / (beta_k + eps))^2, d = (0.1, 0.6, 0.3).
+// The common factor 13/12 of the betas cancels in tau5 / beta except against
+// the FP32 epsilon (1e-30, an effective 1.08e-30); the smoothness ratio is
+// capped at 1e15 as in the scalar FP32 form.
 __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& qr, f2& ql) {
-    const f2 c1 = S2(13.0f / 12.0f), c2 = S2(0.25f);
-    f2 t = fma(S2(-2.0f), qm1, add(qm2, q0));
-    f2 u = fma(S2(-4.0f), qm1, fma(S2(3.0f), q0, qm2));
-    const f2 b1 = fma(mul(c1, t), t, mul(mul(c2, u), u));
-    t = fma(S2(-2.0f), q0, add(qm1, qp1));
-    u = sub(qm1, qp1);
-    const f2 b2 = fma(mul(c1, t), t, mul(mul(c2, u), u));
-    t = fma(S2(-2.0f), qp1, add(qp2, q0));
-    u = fma(S2(-4.0f), qp1, fma(S2(3.0f), q0, qp2));
-    const f2 b3 = fma(mul(c1, t), t, mul(mul(c2, u), u));
+    const f2 D1 = sub(qm1, qm2), D2 = sub(q0, qm1), D3 = sub(qp1, q0), D4 = sub(qp2, qp1);
+    const f2 r = S2(3.0f / 13.0f);
+    f2 t = sub(D2, D1);           // q_im2 + q_i - 2 q_im1
+    f2 u = fma(S2(2.0f), D2, t);  // q_im2 + 3 q_i - 4 q_im1
+    const f2 b1 = fma(mul(r, u), u, mul(t, t));
+    t = sub(D3, D2);  // q_im1 + q_ip1 - 2 q_i
+    u = add(D2, D3);  // q_ip1 - q_im1
+    const f2 b2 = fma(mul(r, u), u, mul(t, t));
+    t = sub(D4, D3);               // q_ip2 + q_i - 2 q_ip1
+    u = fma(S2(-2.0f), D3, t);     // q_ip2 + 3 q_i - 4 q_ip1
+    const f2 b3 = fma(mul(r, u), u, mul(t, t));
     const f2 eps = S2(1.0e-30f);
     const f2 tau = vabs(sub(b1, b3));
     f2 i1 = mul(tau, rcp(add(b1, eps)));
@@ -92,22 +99,25 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
     i3 = P2(fminf(i3.x, 1.0e15f), fminf(i3.y, 1.0e15f));
     const f2 one = S2(1.0f);
     const f2 s1 = fma(i1, i1, one), s2 = fma(i2, i2, one), s3 = fma(i3, i3, one);
-    const f2 a2 = mul(S2(0.6f), s2);
-    // right face of cell i (left-biased stencils)
+    // right face of cell i (left-biased stencils), weights d_k folded into g_k:
+    // 0.1 g1 = 0.1 (5 D2 - 2 D1) / 6, 0.6 g2 = 0.6 (D2 + 2 D3) / 6, 0.3 g3 = 0.3 (4 D3 - D4) / 6
     {
-        const f2 a1 = mul(S2(0.1f), s1), a3 = mul(S2(0.3f), s3);
-        const f2 f1 = fma(S2(11.0f / 6.0f), q0, fma(S2(-7.0f / 6.0f), qm1, mul(S2(2.0f / 6.0f), qm2)));
-        const f2 f2_ = fma(S2(2.0f / 6.0f), qp1, fma(S2(5.0f / 6.0f), q0, mul(S2(-1.0f / 6.0f), qm1)));
-        const f2 f3 = fma(S2(-1.0f / 6.0f), qp2, fma(S2(5.0f / 6.0f), qp1, mul(S2(2.0f / 6.0f), q0)));
-        ql = mul(fma(f3, a3, fma(f2_, a2, mul(f1, a1))), rcp(add(add(a1, a2), a3)));
+        const f2 g1 = fma(S2(0.5f / 6.0f), D2, mul(S2(-0.2f / 6.0f), D1));
+        const f2 g2 = fma(S2(1.2f / 6.0f), D3, mul(S2(0.6f / 6.0f), D2));
+        const f2 g3 = fma(S2(1.2f / 6.0f), D3, mul(S2(-0.3f / 6.0f), D4));
+        const f2 num = fma(s3, g3, fma(s2, g2, mul(s1, g1)));
+        const f2 den = fma(S2(0.3f), s3, fma(S2(0.6f), s2, mul(S2(0.1f), s1)));
+        ql = fma(num, rcp(den), q0);
     }
-    // left face of cell i (right-biased stencils)
+    // left face of cell i (right-biased stencils), d = (0.1, 0.6, 0.3) on (s3, s2, s1):
+    // 0.1 (2 D4 - 5 D3) / 6, 0.6 (-D3 - 2 D2) / 6, 0.3 (D1 - 4 D2) / 6
     {
-        const f2 a1 = mul(S2(0.1f), s3), a3 = mul(S2(0.3f), s1);
-        const f2 f1 = fma(S2(11.0f / 6.0f), q0, fma(S2(-7.0f / 6.0f), qp1, mul(S2(2.0f / 6.0f), qp2)));
-        const f2 f2_ = fma(S2(2.0f / 6.0f), qm1, fma(S2(5.0f / 6.0f), q0, mul(S2(-1.0f / 6.0f), qp1)));
-        const f2 f3 = fma(S2(-1.0f / 6.0f), qm2, fma(S2(5.0f / 6.0f), qm1, mul(S2(2.0f / 6.0f), q0)));
-        qr = mul(fma(f3, a3, fma(f2_, a2, mul(f1, a1))), rcp(add(add(a1, a2), a3)));
+        const f2 g1 = fma(S2(0.2f / 6.0f), D4, mul(S2(-0.5f / 6.0f), D3));
+        const f2 g2 = fma(S2(-1.2f / 6.0f), D2, mul(S2(-0.6f / 6.0f), D3));
+        const f2 g3 = fma(S2(-1.2f / 6.0f), D2, mul(S2(0.3f / 6.0f), D1));
+        const f2 num = fma(s1, g3, fma(s2, g2, mul(s3, g1)));
+        const f2 den = fma(S2(0.3f), s1, fma(S2(0.6f), s2, mul(S2(0.1f), s3)));
+        qr = fma(num, rcp(den), q0);
     }
 }
 
