@@ -133,6 +133,39 @@ int vb_store_prims_host(vb_handle h, double* P_aos_host, void* stream);
 /* Current conserved state U in the reference layout (device pointer). */
 int vb_store_cons(vb_handle h, double* U_aos_dev, void* stream);
 
+/* Initial conditions generated on the device, replacing the examples' host
+ * loops over every cell (examples/Jet3D/HARM_jet_breakout.jl:72-118,
+ * examples/Jet2D/HARM_jet_breakout.jl:37-72) followed by the upload. Every
+ * cell, ghosts included, gets P; then U = PtoU(P) as vb_load_prims does.
+ * The density noise is a standard normal per cell from (seed, padded linear
+ * cell index): splitmix64 words and Box-Muller, reproducible for any launch
+ * shape (the examples draw from per-thread MersenneTwister streams, whose
+ * values depend on the thread schedule). */
+enum {
+    VB_IC_AMBIENT = 0, /* rho (1 + noise N(0,1)), u, zero velocity on every cell; any dims */
+    VB_IC_STAR_JET = 1 /* the examples' stellar envelope with a jet engine; 2D and 3D */
+};
+typedef struct vb_ic_params {
+    uint32_t version; /* VB_ABI_VERSION */
+    int32_t kind;     /* VB_IC_* */
+    uint64_t seed;
+    double noise;     /* relative density noise (the examples: 3e-2) */
+    double rho, u;    /* AMBIENT: density and internal energy density */
+    /* STAR_JET: cell (i, j, k) (1-based over the padded grid) sits at X = i dx,
+     * Y = j dy - box_Y, Z = k dz - box_Z with dx = box_X / (Nx + 6),
+     * dy = 2 box_Y / (Ny + 6), dz = 2 box_Z / (Nz + 6); R = |(X, Y[, Z])|.
+     * rho = rho0 (r_max / max(R, r_eng))^2 (1 + noise N) for R < r_max, else
+     * outer; u = temp rho. For R < r_eng: rho *= engine_rho, u = engine_temp rho,
+     * u^x = gamma0 / (1 - 1/gamma0^2) / cosh(s / r_eng)^8 with s = sqrt(X^2 + Y^2)
+     * in 3D and s = Y in 2D (the examples' expressions). */
+    double box[3];
+    double r_max, r_eng, rho0, temp, outer, gamma0, engine_rho, engine_temp;
+    double reserved_d[4];
+} vb_ic_params;
+/* Fill *ic with the example values for dims (2 or 3; AMBIENT: rho 1, u 3e-3). */
+int vb_default_ic(int dims, int kind, vb_ic_params* ic);
+int vb_init_prims(vb_handle h, const vb_ic_params* ic, void* stream);
+
 /* Run nsteps iterations of the HARM_HLL time-loop body (src/3dim/algos.jl:274-329):
  * boundary fill, the RK stages, t += dt. */
 int vb_step(vb_handle h, double dt, int nsteps, void* stream);

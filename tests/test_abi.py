@@ -100,3 +100,17 @@ def test_grid_entry_points_reject_bad_arguments_without_a_gpu():
     assert b"axis 2" in lib.vb_grid_last_error()
     assert lib.vb_grid_limit(4, 8, 8, 8, None, 0.0, None) == L.ERR_ARG
     assert b"dims 4" in lib.vb_grid_last_error()
+
+
+def test_default_ic_is_the_examples():
+    import ctypes as C
+
+    from verona_b200 import _lib
+
+    ic = _lib.VBIcParams()
+    assert _lib.lib().vb_default_ic(3, 1, C.byref(ic)) == 0
+    assert (ic.version, ic.kind, ic.seed, ic.noise) == (_lib.ABI_VERSION, 1, 42, 3e-2)
+    assert tuple(ic.box) == (480.0, 120.0, 120.0) and ic.r_eng == 5.0 and ic.engine_rho == 1e-2
+    assert _lib.lib().vb_default_ic(2, 1, C.byref(ic)) == 0
+    assert tuple(ic.box)[:2] == (800.0, 200.0) and ic.r_eng == 2.0 and ic.engine_rho == 1e-3
+    assert _lib.lib().vb_default_ic(3, 5, C.byref(ic)) == -1  # VB_ERR_ARG

@@ -150,3 +150,32 @@ def test_oracle_3d_con2prim_floors_like_the_reference(oracle):
     U = oracle.prim2con(3, g, P)
     Q, r = oracle.con2prim(3, g, 50, 1e-12, U, P)
     assert r >= 1 and Q[1] == 1e-8
+
+
+def test_ic_noise_stream_is_standard_normal_and_reproducible():
+    """The counter-based noise of the initial conditions: N(0, 1) moments,
+    no correlation between neighbouring cells, the same values for the same
+    (seed, cell) and different ones for another seed."""
+    from oracle import ic
+
+    c = np.arange(1 << 20, dtype=np.uint64)
+    z = ic.cell_normal(42, c)
+    assert abs(z.mean()) < 5e-3 and abs(z.std() - 1.0) < 5e-3
+    assert abs(np.corrcoef(z[:-1], z[1:])[0, 1]) < 5e-3
+    assert np.array_equal(z[1000:2000], ic.cell_normal(42, c[1000:2000]))
+    assert np.mean(np.abs(z - ic.cell_normal(43, c))) > 0.5
+
+
+def test_ic_star_jet_follows_the_examples():
+    """Engine region, envelope and outer medium of the 3D example's initial
+    condition (examples/Jet3D/HARM_jet_breakout.jl:82-114) on a small grid."""
+    from oracle import ic
+
+    P = ic.star_jet(3, (58, 26, 26))  # 64 x 32 x 32 padded: dx = 7.5
+    rho, u, ux = P[0], P[1], P[2]
+    assert np.all(P[3] == 0) and np.all(P[4] == 0)
+    assert np.all(rho > 0) and np.all(u > 0)
+    # cell (1,16,16) 1-based: X = 7.5, Y = Z = 0 -> inside R_max, outside R_eng (5): no jet
+    assert ux[0, 15, 15] == 0.0 and abs(rho[0, 15, 15] / (2.5e-2 * (100 / 7.5) ** 2) - 1) < 0.2
+    assert np.all(rho[-1] == 1e-4)  # X = 480 is outside R_max
+    assert np.allclose(u[rho == 1e-4], 1e-9)

@@ -47,6 +47,17 @@ class VBTuning(C.Structure):
                 ("fp32_pairs", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
+class VBIcParams(C.Structure):
+    _fields_ = [("version", C.c_uint32), ("kind", C.c_int32), ("seed", C.c_uint64), ("noise", C.c_double),
+                ("rho", C.c_double), ("u", C.c_double), ("box", C.c_double * 3), ("r_max", C.c_double),
+                ("r_eng", C.c_double), ("rho0", C.c_double), ("temp", C.c_double), ("outer", C.c_double),
+                ("gamma0", C.c_double), ("engine_rho", C.c_double), ("engine_temp", C.c_double),
+                ("reserved_d", C.c_double * 4)]
+
+
+IC_KINDS = {"ambient": 0, "star_jet": 1}
+
+
 class VBError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"verona_b200 error {code}: {msg}")
@@ -70,6 +81,8 @@ _SIGS = {
     "vb_load_prims_host": [_vp, _vp, _vp],
     "vb_store_prims_host": [_vp, _vp, _vp],
     "vb_store_cons": [_vp, _vp, _vp],
+    "vb_default_ic": [C.c_int, C.c_int, C.POINTER(VBIcParams)],
+    "vb_init_prims": [_vp, C.POINTER(VBIcParams), _vp],
     "vb_step": [_vp, C.c_double, C.c_int, _vp],
     "vb_get_time": [_vp, _dp],
     "vb_set_time": [_vp, C.c_double],

@@ -352,6 +352,76 @@ int vb_store_cons(vb_handle h, double* Ua, void* stream) {
     return VB_OK;
 }
 
+int vb_default_ic(int dims, int kind, vb_ic_params* ic) {
+    if (!ic || dims < 1 || dims > 3 || kind < VB_IC_AMBIENT || kind > VB_IC_STAR_JET)
+        return fail(nullptr, VB_ERR_ARG, "vb_default_ic: bad argument");
+    *ic = vb_ic_params{};
+    ic->version = VB_ABI_VERSION;
+    ic->kind = kind;
+    ic->seed = 42;  // the examples' seed
+    ic->noise = 3e-2;
+    ic->rho = 1.0;
+    ic->u = 3e-3;
+    if (dims == 3) {  // examples/Jet3D/HARM_jet_breakout.jl:46-61
+        ic->box[0] = 480.0;
+        ic->box[1] = 120.0;
+        ic->box[2] = 120.0;
+        ic->r_eng = 5.0;
+        ic->engine_rho = 1e-2;
+    } else {  // examples/Jet2D/HARM_jet_breakout.jl:26-36
+        ic->box[0] = 800.0;
+        ic->box[1] = 200.0;
+        ic->box[2] = 0.0;
+        ic->r_eng = 2.0;
+        ic->engine_rho = 1e-3;
+    }
+    ic->r_max = 100.0;
+    ic->rho0 = 2.5e-2;
+    ic->temp = 1e-5;
+    ic->outer = 1e-4;
+    ic->gamma0 = 10.0;
+    ic->engine_temp = 1e-5;
+    return VB_OK;
+}
+
+int vb_init_prims(vb_handle h, const vb_ic_params* ic, void* stream) {
+    if (!h || !ic) return fail(h, VB_ERR_ARG, "vb_init_prims: null argument");
+    if (ic->version != VB_ABI_VERSION) return fail(h, VB_ERR_ARG, "vb_init_prims: version %u", ic->version);
+    if (h->nghost == 0) return fail(h, VB_ERR_UNSUPPORTED, "vb_init_prims: the 1D reference layout loads host arrays");
+    if (ic->kind != VB_IC_AMBIENT && ic->kind != VB_IC_STAR_JET)
+        return fail(h, VB_ERR_ARG, "vb_init_prims: kind %d", ic->kind);
+    if (ic->kind == VB_IC_STAR_JET && h->dims < 2)
+        return fail(h, VB_ERR_UNSUPPORTED, "vb_init_prims: the star + jet condition is 2D or 3D");
+    if (ic->kind == VB_IC_STAR_JET && (!(ic->r_eng > 0.0) || !(ic->r_max > 0.0) || !(ic->gamma0 > 1.0)))
+        return fail(h, VB_ERR_ARG, "vb_init_prims: r_eng, r_max > 0 and gamma0 > 1 required");
+    InitIC c{};
+    c.kind = ic->kind;
+    c.seed = ic->seed;
+    c.noise = ic->noise;
+    c.rho = ic->rho;
+    c.u = ic->u;
+    for (int a = 0; a < 3; ++a) {
+        c.box[a] = ic->box[a];
+        c.dx[a] = (a == 0 ? 1.0 : 2.0) * ic->box[a] / (double)h->np[a];
+    }
+    c.r_max = ic->r_max;
+    c.r_eng = ic->r_eng;
+    c.rho0 = ic->rho0;
+    c.temp = ic->temp;
+    c.outer = ic->outer;
+    c.gamma0 = ic->gamma0;
+    c.engine_rho = ic->engine_rho;
+    c.engine_temp = ic->engine_temp;
+    cudaStream_t s = (cudaStream_t)stream;
+    Grid g = grid_of(h);
+    if (fp32(h))
+        VB_CUDA(h, launch_init_prims<float>(g, c, (float*)h->P[h->cur], h->U0, h->gamma, s));
+    else
+        VB_CUDA(h, launch_init_prims<double>(g, c, (double*)h->P[h->cur], h->U0, h->gamma, s));
+    h->loaded = true;
+    return VB_OK;
+}
+
 }  // extern "C"
 
 static int prof_events(vb_handle h, cudaEvent_t* a, cudaEvent_t* b) {

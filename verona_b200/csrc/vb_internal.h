@@ -69,6 +69,16 @@ cudaError_t launch_load_prims(const Grid& g, const double* P_aos, R* P, double* 
                               cudaStream_t s);
 template <typename R>
 cudaError_t launch_store_prims(const Grid& g, const R* P, double* P_aos, cudaStream_t s);
+// initial condition generated on the device (vb_init_prims): P on every cell, U0 = PtoU(P)
+struct InitIC {
+    int kind;  // 0 ambient, 1 star + jet engine
+    unsigned long long seed;
+    double noise, rho, u;
+    double dx[3], box[3];
+    double r_max, r_eng, rho0, temp, outer, gamma0, engine_rho, engine_temp;
+};
+template <typename R>
+cudaError_t launch_init_prims(const Grid& g, const InitIC& ic, R* P, double* U0, double gamma, cudaStream_t s);
 // ghost cells of Pout = limit(ghost cells of Pin)
 template <typename R>
 cudaError_t launch_ghost_limit(const Grid& g, const R* Pin, R* Pout, double floor_, cudaStream_t s);

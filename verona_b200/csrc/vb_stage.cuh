@@ -345,6 +345,79 @@ __global__ void k_store_prims(Grid g, const R* __restrict__ P, double* __restric
     }
 }
 
+// ---- device initial conditions ----------------------------------------------
+// splitmix64 (Steele, Lea, Flood 2014; constants of Vigna's reference
+// implementation): a bijective 64-bit mixer, used as a counter-based stream.
+__host__ __device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+// standard normal deviate of cell c in stream `seed` (Box-Muller on two words)
+__device__ __forceinline__ double cell_normal(unsigned long long seed, unsigned long long c) {
+    const unsigned long long h1 = splitmix64(seed ^ splitmix64(2 * c));
+    const unsigned long long h2 = splitmix64(seed ^ splitmix64(2 * c + 1));
+    const double u1 = (double)((h1 >> 11) + 1) * 0x1.0p-53;  // (0, 1]
+    const double u2 = (double)(h2 >> 11) * 0x1.0p-53;        // [0, 1)
+    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+}
+
+// The examples' initial conditions (examples/Jet3D/HARM_jet_breakout.jl:72-118,
+// examples/Jet2D/HARM_jet_breakout.jl:37-72) or an ambient medium, on every
+// padded cell; then the tail of k_load_prims.
+template <int DIM, typename R>
+__global__ void k_init_prims(Grid g, InitIC ic, R* __restrict__ P, double* __restrict__ U0, double gamma) {
+    constexpr int NV = 2 + DIM;
+    const long long ncell = (long long)g.n[0] * g.n[1] * g.n[2];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        double q[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) q[v] = 0.0;
+        const double nz = ic.noise * cell_normal(ic.seed, (unsigned long long)c);
+        if (ic.kind == 0) {
+            q[0] = ic.rho * (1.0 + nz);
+            q[1] = ic.u;
+        } else {
+            const int i = (int)(c % g.n[0]);
+            const int j = (int)((c / g.n[0]) % g.n[1]);
+            const int k = (int)(c / ((long long)g.n[0] * g.n[1]));
+            const double X = (i + 1) * ic.dx[0];
+            const double Y = (j + 1) * ic.dx[1] - ic.box[1];
+            const double Z = DIM > 2 ? (k + 1) * ic.dx[2] - ic.box[2] : 0.0;
+            const double R2 = DIM > 2 ? X * X + Y * Y + Z * Z : X * X + Y * Y;
+            const double Rr = sqrt(R2);
+            double rho;
+            if (Rr < ic.r_max) {
+                const double f = ic.r_max / (Rr < ic.r_eng ? ic.r_eng : Rr);
+                rho = ic.rho0 * (f * f) * (1.0 + nz);
+            } else {
+                rho = ic.outer;
+            }
+            double u = rho * ic.temp;
+            if (Rr < ic.r_eng) {
+                const double s = DIM > 2 ? sqrt(X * X + Y * Y) : Y;
+                const double ch = cosh(s / ic.r_eng);
+                const double ch2 = ch * ch, ch4 = ch2 * ch2;
+                const double v = 1.0 / (1.0 - 1.0 / (ic.gamma0 * ic.gamma0)) * (1.0 / (ch4 * ch4));
+                q[2] = ic.gamma0 * v;
+                rho = rho * ic.engine_rho;
+                u = rho * ic.engine_temp;
+            }
+            q[0] = rho;
+            q[1] = u;
+        }
+        double uc[NV];
+        prim2con<DIM>(gamma, q, uc);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            P[v * g.vs + c] = (R)q[v];
+            U0[v * g.vs + c] = uc[v];
+        }
+    }
+}
+
 inline int grid_for(long long n, int nt) {
     long long b = (n + nt - 1) / nt;
     if (b > 148LL * 32) b = 148LL * 32;
@@ -358,6 +431,16 @@ cudaError_t launch_load_prims(const Grid& g, const double* Pa, R* P, double* U0,
     if (g.dims == 1) k_load_prims<1, R><<<nb, 256, 0, s>>>(g, Pa, P, U0, gamma);
     else if (g.dims == 2) k_load_prims<2, R><<<nb, 256, 0, s>>>(g, Pa, P, U0, gamma);
     else k_load_prims<3, R><<<nb, 256, 0, s>>>(g, Pa, P, U0, gamma);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_init_prims(const Grid& g, const InitIC& ic, R* P, double* U0, double gamma, cudaStream_t s) {
+    long long ncell = (long long)g.n[0] * g.n[1] * g.n[2];
+    int nb = grid_for(ncell, 256);
+    if (g.dims == 1) k_init_prims<1, R><<<nb, 256, 0, s>>>(g, ic, P, U0, gamma);
+    else if (g.dims == 2) k_init_prims<2, R><<<nb, 256, 0, s>>>(g, ic, P, U0, gamma);
+    else k_init_prims<3, R><<<nb, 256, 0, s>>>(g, ic, P, U0, gamma);
     return cudaGetLastError();
 }
 
@@ -577,6 +660,7 @@ cudaError_t launch_max_speed(const Grid& g, const R* P, double gamma, double* pa
     template cudaError_t launch_load_prims<R>(const Grid&, const double*, R*, double*, double,        \
                                               cudaStream_t);                                          \
     template cudaError_t launch_store_prims<R>(const Grid&, const R*, double*, cudaStream_t);        \
+    template cudaError_t launch_init_prims<R>(const Grid&, const InitIC&, R*, double*, double, cudaStream_t); \
     template cudaError_t launch_ghost_limit<R>(const Grid&, const R*, R*, double, cudaStream_t);      \
     template cudaError_t launch_bc_face<R>(const Grid&, R*, int, int, const double*, cudaStream_t);  \
     template cudaError_t launch_bc_decay<R>(const Grid&, R*, int, int, double, cudaStream_t);        \

@@ -75,6 +75,23 @@ class Solver:
             self._check_dev(P)
             L.check(L.lib().vb_load_prims(self._h, C.c_void_p(P.data_ptr()), _stream_ptr(stream)), self._h)
 
+    def init_prims(self, kind: str = "star_jet", stream=None, **params):
+        """Generate the initial condition on the device (vb_init_prims): the
+        examples' star + jet engine ("star_jet", 2D/3D) or an ambient medium
+        ("ambient"); keyword arguments override the example values
+        (seed, noise, rho, u, box, r_max, r_eng, rho0, temp, outer, gamma0,
+        engine_rho, engine_temp). Returns the parameters used."""
+        ic = L.VBIcParams()
+        L.check(L.lib().vb_default_ic(self.dims, L.IC_KINDS[kind], C.byref(ic)))
+        for k, v in params.items():
+            if k == "box":
+                for a, x in enumerate(v):
+                    ic.box[a] = float(x)
+            else:
+                setattr(ic, k, v)
+        L.check(L.lib().vb_init_prims(self._h, C.byref(ic), _stream_ptr(stream)), self._h)
+        return ic
+
     def store_prims(self, out=None, stream=None):
         """Device tensor `out` (or a new one) filled with the current P."""
         import torch
