@@ -162,6 +162,22 @@ typedef struct vb_ic_params {
     double r_max, r_eng, rho0, temp, outer, gamma0, engine_rho, engine_temp;
     double reserved_d[4];
 } vb_ic_params;
+/* Asynchronous dump of the interior primitives, the data of the reference's
+ * SaveHDF5Gather / SaveHDF5Parallel (src/3dim/saving.jl:1-146:
+ * Array(P.arr[:, 4:end-3, 4:end-3, 4:end-3]) and its NaN check); the caller
+ * writes the HDF5 file ("data", plus "T" / "grid") as the reference does.
+ * vb_dump_begin: at this point of `stream` the interior P is packed into
+ * host_out's layout, (nvar, Nx, Ny[, Nz]) FP64 column-major, in a device
+ * buffer of the handle (allocated on the first dump), and copied to host_out
+ * on a copy stream of the handle while later work on `stream` (vb_step)
+ * proceeds; host_out must stay valid until vb_dump_wait and should be pinned
+ * (a pageable buffer makes the copy synchronous). The NaN values of the
+ * snapshot are counted on the device. vb_dump_wait blocks until the copy has
+ * landed and returns that count. One dump in flight per handle: a second
+ * vb_dump_begin orders itself after the previous copy. */
+int vb_dump_begin(vb_handle h, double* host_out, void* stream);
+int vb_dump_wait(vb_handle h, uint64_t* nan_count);
+
 /* Fill *ic with the example values for dims (2 or 3; AMBIENT: rho 1, u 3e-3). */
 int vb_default_ic(int dims, int kind, vb_ic_params* ic);
 int vb_init_prims(vb_handle h, const vb_ic_params* ic, void* stream);

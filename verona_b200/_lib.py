@@ -83,6 +83,8 @@ _SIGS = {
     "vb_store_cons": [_vp, _vp, _vp],
     "vb_default_ic": [C.c_int, C.c_int, C.POINTER(VBIcParams)],
     "vb_init_prims": [_vp, C.POINTER(VBIcParams), _vp],
+    "vb_dump_begin": [_vp, _vp, _vp],
+    "vb_dump_wait": [_vp, C.POINTER(C.c_uint64)],
     "vb_step": [_vp, C.c_double, C.c_int, _vp],
     "vb_get_time": [_vp, _dp],
     "vb_set_time": [_vp, C.c_double],

@@ -58,6 +58,13 @@ struct vb_solver {
     const void* mlp_blob = nullptr;
     unsigned int* tc_err = nullptr;
     float* w_guess = nullptr;  // one W guess per padded cell
+    // asynchronous dumps (vb_dump_begin / vb_dump_wait)
+    double* dump_buf = nullptr;            // interior snapshot, reference interior layout
+    unsigned long long* dump_nan = nullptr;  // device NaN count of the snapshot
+    unsigned long long* dump_nan_host = nullptr;  // pinned
+    cudaStream_t dump_stream = nullptr;
+    cudaEvent_t dump_packed = nullptr, dump_copied = nullptr;
+    bool dump_pending = false;
     // profiling
     bool prof = false;
     std::vector<cudaEvent_t> ev;
@@ -146,6 +153,13 @@ int vb_destroy(vb_handle h) {
     cudaFree(h->staging);
     cudaFree(h->tc_err);
     cudaFree(h->w_guess);
+    if (h->dump_stream) cudaStreamSynchronize(h->dump_stream);
+    cudaFree(h->dump_buf);
+    cudaFree(h->dump_nan);
+    cudaFreeHost(h->dump_nan_host);
+    if (h->dump_packed) cudaEventDestroy(h->dump_packed);
+    if (h->dump_copied) cudaEventDestroy(h->dump_copied);
+    if (h->dump_stream) cudaStreamDestroy(h->dump_stream);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     cudaSetDevice(prev);
     delete h;
@@ -349,6 +363,52 @@ int vb_store_cons(vb_handle h, double* Ua, void* stream) {
     } else {
         VB_CUDA(h, launch_store_prims<double>(grid_of(h), h->U0, Ua, s));
     }
+    return VB_OK;
+}
+
+static size_t interior_bytes(const vb_solver* h) {
+    return sizeof(double) * h->nv * (size_t)h->n[0] * h->n[1] * h->n[2];
+}
+
+int vb_dump_begin(vb_handle h, double* host_out, void* stream) {
+    if (!h || !host_out) return fail(h, VB_ERR_ARG, "vb_dump_begin: null argument");
+    if (h->nghost == 0) return fail(h, VB_ERR_UNSUPPORTED, "vb_dump_begin: the 1D reference layout stores with vb_store_prims_host");
+    if (!h->loaded) return fail(h, VB_ERR_STATE, "vb_dump_begin: no state loaded");
+    if (!h->dump_buf) {
+        int rc = dev_alloc(h, (void**)&h->dump_buf, interior_bytes(h));
+        if (rc) return rc;
+        rc = dev_alloc(h, (void**)&h->dump_nan, sizeof(unsigned long long));
+        if (rc) return rc;
+        VB_CUDA(h, cudaMallocHost((void**)&h->dump_nan_host, sizeof(unsigned long long)));
+        VB_CUDA(h, cudaStreamCreateWithFlags(&h->dump_stream, cudaStreamNonBlocking));
+        VB_CUDA(h, cudaEventCreateWithFlags(&h->dump_packed, cudaEventDisableTiming));
+        VB_CUDA(h, cudaEventCreateWithFlags(&h->dump_copied, cudaEventDisableTiming));
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    // the previous dump's copy must have read the snapshot buffer before it is overwritten
+    if (h->dump_pending) VB_CUDA(h, cudaStreamWaitEvent(s, h->dump_copied, 0));
+    VB_CUDA(h, cudaMemsetAsync(h->dump_nan, 0, sizeof(unsigned long long), s));
+    Grid g = grid_of(h);
+    if (fp32(h))
+        VB_CUDA(h, launch_pack_interior<float>(g, (const float*)h->P[h->cur], h->dump_buf, h->dump_nan, s));
+    else
+        VB_CUDA(h, launch_pack_interior<double>(g, (const double*)h->P[h->cur], h->dump_buf, h->dump_nan, s));
+    VB_CUDA(h, cudaEventRecord(h->dump_packed, s));
+    VB_CUDA(h, cudaStreamWaitEvent(h->dump_stream, h->dump_packed, 0));
+    VB_CUDA(h, cudaMemcpyAsync(host_out, h->dump_buf, interior_bytes(h), cudaMemcpyDeviceToHost, h->dump_stream));
+    VB_CUDA(h, cudaMemcpyAsync(h->dump_nan_host, h->dump_nan, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                               h->dump_stream));
+    VB_CUDA(h, cudaEventRecord(h->dump_copied, h->dump_stream));
+    h->dump_pending = true;
+    return VB_OK;
+}
+
+int vb_dump_wait(vb_handle h, uint64_t* nan_count) {
+    if (!h) return fail(nullptr, VB_ERR_ARG, "vb_dump_wait: null handle");
+    if (!h->dump_pending) return fail(h, VB_ERR_STATE, "vb_dump_wait: no dump in flight");
+    VB_CUDA(h, cudaEventSynchronize(h->dump_copied));
+    h->dump_pending = false;
+    if (nan_count) *nan_count = *h->dump_nan_host;
     return VB_OK;
 }
 

@@ -69,6 +69,11 @@ cudaError_t launch_load_prims(const Grid& g, const double* P_aos, R* P, double* 
                               cudaStream_t s);
 template <typename R>
 cudaError_t launch_store_prims(const Grid& g, const R* P, double* P_aos, cudaStream_t s);
+// interior cells of P -> the reference's interior layout (nvar, Nx, Ny[, Nz]), FP64,
+// column-major, variable fastest; adds the count of NaN values to *nan_count
+template <typename R>
+cudaError_t launch_pack_interior(const Grid& g, const R* P, double* out, unsigned long long* nan_count,
+                                 cudaStream_t s);
 // initial condition generated on the device (vb_init_prims): P on every cell, U0 = PtoU(P)
 struct InitIC {
     int kind;  // 0 ambient, 1 star + jet engine

@@ -434,6 +434,48 @@ cudaError_t launch_load_prims(const Grid& g, const double* Pa, R* P, double* U0,
     return cudaGetLastError();
 }
 
+// Interior snapshot of a dump (src/3dim/saving.jl:57-146 copies
+// P.arr[:, 4:end-3, 4:end-3, 4:end-3] to the host and rejects NaN): one
+// thread per interior cell, x fastest; reads each variable array coalesced,
+// writes the cell's nv consecutive doubles; NaN values counted per warp.
+template <int DIM, typename R>
+__global__ void k_pack_interior(Grid g, const R* __restrict__ P, double* __restrict__ out,
+                                unsigned long long* __restrict__ nan_count) {
+    constexpr int NV = 2 + DIM;
+    const int N0 = g.n[0] - 2 * NG, N1 = DIM > 1 ? g.n[1] - 2 * NG : 1, N2 = DIM > 2 ? g.n[2] - 2 * NG : 1;
+    const long long tot = (long long)N0 * N1 * N2;
+    CellMap cm;
+    cm.init(N0, N1, g.sy, g.sz, NG);
+    const long long off = DIM == 1 ? 0 : (DIM == 2 ? -NG * g.sz : 0);  // 2D: no z ghosts
+    unsigned int nans = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        long long c = cm.padded((uint32_t)e) + off;
+        if (DIM == 1) c -= NG * (g.sy + g.sz);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const double x = (double)P[v * g.vs + c];
+            nans += isnan(x) ? 1u : 0u;
+            out[e * NV + v] = x;
+        }
+    }
+    nans = __reduce_add_sync(0xffffffffu, nans);
+    if ((threadIdx.x & 31) == 0 && nans) atomicAdd(nan_count, (unsigned long long)nans);
+}
+
+template <typename R>
+cudaError_t launch_pack_interior(const Grid& g, const R* P, double* out, unsigned long long* nan_count,
+                                 cudaStream_t s) {
+    const long long tot = (long long)(g.n[0] - 2 * NG) * (g.dims > 1 ? g.n[1] - 2 * NG : 1) *
+                          (g.dims > 2 ? g.n[2] - 2 * NG : 1);
+    if ((unsigned long long)tot > MAX_CELLS_U32) return cudaErrorInvalidValue;
+    const int nb = grid_for(tot, 256);
+    if (g.dims == 1) k_pack_interior<1, R><<<nb, 256, 0, s>>>(g, P, out, nan_count);
+    else if (g.dims == 2) k_pack_interior<2, R><<<nb, 256, 0, s>>>(g, P, out, nan_count);
+    else k_pack_interior<3, R><<<nb, 256, 0, s>>>(g, P, out, nan_count);
+    return cudaGetLastError();
+}
+
 template <typename R>
 cudaError_t launch_init_prims(const Grid& g, const InitIC& ic, R* P, double* U0, double gamma, cudaStream_t s) {
     long long ncell = (long long)g.n[0] * g.n[1] * g.n[2];
@@ -661,6 +703,7 @@ cudaError_t launch_max_speed(const Grid& g, const R* P, double gamma, double* pa
                                               cudaStream_t);                                          \
     template cudaError_t launch_store_prims<R>(const Grid&, const R*, double*, cudaStream_t);        \
     template cudaError_t launch_init_prims<R>(const Grid&, const InitIC&, R*, double*, double, cudaStream_t); \
+    template cudaError_t launch_pack_interior<R>(const Grid&, const R*, double*, unsigned long long*, cudaStream_t); \
     template cudaError_t launch_ghost_limit<R>(const Grid&, const R*, R*, double, cudaStream_t);      \
     template cudaError_t launch_bc_face<R>(const Grid&, R*, int, int, const double*, cudaStream_t);  \
     template cudaError_t launch_bc_decay<R>(const Grid&, R*, int, int, double, cudaStream_t);        \

@@ -92,6 +92,27 @@ class Solver:
         L.check(L.lib().vb_init_prims(self._h, C.byref(ic), _stream_ptr(stream)), self._h)
         return ic
 
+    @property
+    def interior_shape(self):
+        """Fortran-order host shape (nvar, Nx, ...) of a dump."""
+        return (self.nv,) + tuple(self.n[a] for a in range(self.dims))
+
+    def dump_begin(self, out: np.ndarray, stream=None) -> np.ndarray:
+        """Start an asynchronous dump of the interior P into `out` (float64,
+        Fortran order, interior_shape; pinned memory for the copy to overlap
+        later steps). Keep `out` alive until dump_wait."""
+        assert out.dtype == np.float64 and out.flags["F_CONTIGUOUS"] and out.shape == self.interior_shape
+        L.check(L.lib().vb_dump_begin(self._h, out.ctypes.data_as(C.c_void_p), _stream_ptr(stream)), self._h)
+        self._dump_out = out
+        return out
+
+    def dump_wait(self) -> int:
+        """Wait for the dump in flight; returns the number of NaN values in it."""
+        n = C.c_uint64()
+        L.check(L.lib().vb_dump_wait(self._h, C.byref(n)), self._h)
+        self._dump_out = None
+        return int(n.value)
+
     def store_prims(self, out=None, stream=None):
         """Device tensor `out` (or a new one) filled with the current P."""
         import torch
