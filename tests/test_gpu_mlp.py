@@ -191,3 +191,32 @@ def test_learned_fused_kernel_matches_two_kernel_form(net, precision):
     l1 = [float(np.mean(np.abs(a[v] - b[v])) / np.mean(np.abs(b[v]))) for v in (0, 1)]
     print(precision, "z-pair stencil + fused vs one-cell stencil + fused: L1 rho, p", l1)
     assert max(l1) < (1e-12 if precision == "fp64" else 2e-6)
+
+
+def test_w_newton_recovers_the_primitive_state():
+    """vb_point_c2p_w against the exact answer: P -> U = PtoU(P) -> P over the
+    training ranges (Lorentz factor up to 40, below the solver's cap of 50),
+    from a perturbed guess and from the state-only cold start. W stops at a
+    Newton step of 1e-12 W; rho and the four-velocity inherit that error
+    amplified by about Lorentz^2 (Lorentz^3 for u^i), u by the cancellation
+    W / Lorentz^2 - D / Lorentz, and u is floored at 1e-8. The cold start
+    ends in the bracketed phase for about one cell in 40; for cold (p/rho ~
+    4e-6) ultra-relativistic states its root is ill-conditioned and one cell
+    of this sample stops 3.3e-10 W away (the same with IEEE divides), hence the
+    10x looser bound there."""
+    import torch
+
+    from verona_b200 import mlp
+
+    P = mlp.synthetic_states(1 << 16, G, seed=11, lorentz_max=40.0)
+    U = mlp.prim2con_torch(P, G)
+    lor = torch.sqrt(1 + P[2] ** 2 + P[3] ** 2 + P[4] ** 2)
+    W = (P[0] + G * P[1]) * lor**2
+    for W0, slack in ((W * (1 + 1e-3), 1.0), (U[0] - U[1], 10.0)):
+        R, it, fb = mlp.c2p_w(U, W0, G)
+        assert (it > 0).all()
+        er = ((R[0] - P[0]).abs() / P[0] / (slack * 1e-10 * lor**2)).max().item()
+        ev = ((R[2:5] - P[2:5]).abs() / (slack * 1e-10 * lor**3)).max().item()
+        eu = ((R[1] - P[1].clamp(min=1e-8)).abs() / (slack * 1e-9 * W + 2e-8)).max().item()
+        print("normalised errors rho %.3f u^i %.3f u %.3f, mean iterations %.2f" % (er, ev, eu, it.double().mean()))
+        assert er < 1.0 and ev < 1.0 and eu < 1.0

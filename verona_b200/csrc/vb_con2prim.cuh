@@ -441,15 +441,45 @@ static VB_NOINLINE __host__ __device__ int c2p_3d_tail(double g, int n_iter, dou
 struct WRes {
     double f, df;
 };
-VB_HD double rsqrt_d(double x) {
+// Reciprocal and reciprocal square root of the W Newton: the hardware
+// approximations of sm_100a (rcp.approx.ftz.f64, rsqrt.approx.ftz.f64) refined
+// by two Newton-Raphson steps each; a step doubles the correct bits (a 23-bit
+// seed ends within an ulp, checked by emulation), and the recovered states
+// equal those of the IEEE-divide form to the W tolerance on every cell of the
+// exact-answer test of the W Newton:
+//   1/x:       e = 1 - x y,              y <- y + y e
+//   1/sqrt(a): t = 1/2 - (a/2) y^2,      y <- y + y t
+// For positive normal arguments (W, 1 - v^2 > 0 here; a zero or NaN argument
+// gives NaN, which the Newton treats as a failed step). The IEEE divide and
+// square root sequences carry special-case handling this loop does not need;
+// the reference con2prim cascade keeps them.
+VB_HD double rcp_nr(double x) {
 #ifdef __CUDA_ARCH__
-    return rsqrt(x);
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
 #else
-    return 1.0 / sqrt(x);
+    return 1.0 / x;
+#endif
+}
+VB_HD double rsqrt_d(double a) {
+#ifdef __CUDA_ARCH__
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+    const double h = 0.5 * a;
+    double t = fma(-h * y, y, 0.5);
+    y = fma(y, t, y);
+    t = fma(-h * y, y, 0.5);
+    return fma(y, t, y);
+#else
+    return 1.0 / sqrt(a);
 #endif
 }
 VB_HD WRes w_residual(double k, double D, double Q_t, double S2, double W) {
-    const double iW = 1.0 / W;
+    const double iW = rcp_nr(W);
     double v2 = S2 * iW * iW;
     if (v2 > 1.0 - 1e-15) v2 = 1.0 - 1e-15;
     const double a = 1.0 - v2;
@@ -464,13 +494,13 @@ VB_HD WRes w_residual(double k, double D, double Q_t, double S2, double W) {
 // 1/W and 1/sqrt(1 - v^2) (the W Newton's refinement, not the reference
 // cascade, whose prims_from_W keeps the reference's operation order).
 VB_HD void prims_from_W_fast(double g, double D, double Qx, double Qy, double Qz, double S2, double W, double* P) {
-    const double iW = 1.0 / W;
+    const double iW = rcp_nr(W);
     const double a = 1.0 - S2 * iW * iW;
     const double rs = rsqrt_d(a);
     const double gm = jmin(rs, 50.0);
     const double igm = gm < rs ? 1.0 / 50.0 : a * rs;  // 1 / gm
     P[0] = jmax(1e-8, D * igm);
-    P[1] = jmax(1e-8, (W * igm * igm - D * igm) / g);
+    P[1] = jmax(1e-8, (W * igm * igm - D * igm) * rcp_nr(g));
     const double f = gm * iW;
     P[2] = Qx * f;
     P[3] = Qy * f;
@@ -496,7 +526,7 @@ VB_HD int c2p_w(double g, const double* Uc, double W0, double rtol, int max_newt
     if (!(W > Wlo0) || !isfinite(W)) W = fmax(Wlo0 * 1.0000001, D - Q_t);
     for (; it < max_newton; ++it) {
         WRes r = w_residual(k, D, Q_t, S2, W);
-        double dW = r.f / r.df;
+        double dW = r.f * rcp_nr(r.df);
         double Wn = W - dW;
         if (!(Wn > Wlo0)) Wn = 0.5 * (W + Wlo0);
         bool done = fabs(Wn - W) <= rtol * fabs(Wn);
