@@ -126,7 +126,7 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
 // Sign convention of the energy slot: E = -U[1] > 0 and FE = -F[1].
 template <int D> struct Side {
     f2 P[5];
-    f2 gam, gw, uw, vn, p, lp, lm;
+    f2 gam, gw, uw, vn, p, np, lp, lm;
     __device__ __forceinline__ void make(f2 g, f2 gm1, const f2* Pin) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) P[v] = Pin[v];
@@ -139,9 +139,11 @@ template <int D> struct Side {
         const f2 igam = rcp(gam);
         vn = mul(un, igam);
         p = mul(gm1, P[1]);
-        // C^2 = Gamma (Gamma - 1) u / (rho + Gamma u) = Gamma p / w  (SoundSpeed, src/eos.jl:15-21)
-        const f2 C2 = mul(mul(g, p), rcp(w));
-        const f2 sig = mul(C2, mul(mul(igam, igam), rcp(sub(one, C2))));
+        np = mul(S2(-1.0f), p);
+        // C^2 = Gamma (Gamma - 1) u / (rho + Gamma u) = Gamma p / w  (SoundSpeed, src/eos.jl:15-21), so
+        // sig = C^2 / (gam^2 (1 - C^2)) = Gamma p / (gam^2 (w - Gamma p)), w - Gamma p > 0: one reciprocal
+        const f2 gp = mul(g, p);
+        const f2 sig = mul(mul(gp, mul(igam, igam)), rcp(sub(w, gp)));
         const f2 r = vsqrt(mul(sig, add(sub(one, mul(vn, vn)), sig)));
         const f2 inv = rcp(add(one, sig));
         lp = mul(add(vn, r), inv);
@@ -150,7 +152,7 @@ template <int D> struct Side {
     // conserved component v in the energy-positive convention (slot 1 = E)
     __device__ __forceinline__ f2 U(int v) const {
         if (v == 0) return mul(gam, P[0]);
-        if (v == 1) return fma(gam, gw, mul(S2(-1.0f), p));
+        if (v == 1) return fma(gam, gw, np);
         return mul(P[v], gw);
     }
     // flux component v along D, energy slot = FE
@@ -172,14 +174,13 @@ __device__ __forceinline__ void face_flux(f2 g, f2 gm1, const f2* PL, const f2* 
     const f2 lR = vmax(L.lp, R.lp);  // Cmax
     const f2 lL = vmin(L.lm, R.lm);  // -Cmin
     const f2 idl = rcp(sub(lR, lL));
-    const f2 lRL = mul(lR, lL);
     const m2 use_R{lR.x < 0.0f, lR.y < 0.0f};
     const m2 use_L{!use_R.x && lL.x > 0.0f, !use_R.y && lL.y > 0.0f};
-    // HLL flux, energy-positive convention
+    // HLL flux, energy-positive convention: (lR F_L - lL F_R + lR lL (U_R - U_L)) / (lR - lL)
+    const f2 cL = mul(lR, idl), cR = mul(mul(S2(-1.0f), lL), idl), cU = mul(mul(lR, lL), idl);
     f2 Fh[5];
 #pragma unroll
-    for (int v = 0; v < 5; ++v)
-        Fh[v] = mul(fma(lRL, sub(R.U(v), L.U(v)), fma(lR, L.F(v), mul(mul(S2(-1.0f), lL), R.F(v)))), idl);
+    for (int v = 0; v < 5; ++v) Fh[v] = fma(cU, sub(R.U(v), L.U(v)), fma(cL, L.F(v), mul(cR, R.F(v))));
     if (RS == RS_HLL) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
@@ -205,20 +206,20 @@ __device__ __forceinline__ void face_flux(f2 g, f2 gm1, const f2* PL, const f2* 
     const f2 ilk = rcp(sub(lK, ls));
     const f2 dv = sub(lK, vn);
     const f2 fac = mul(dv, ilk);
+    const f2 lkf = mul(lK, sub(fac, S2(1.0f)));  // star flux of a passive component: F + lK (fac - 1) U
     const m2 use_hll{!use_R.x && !use_L.x && (!(ps.x > 0.0f) || !(ls.x >= lL.x && ls.x <= lR.x)),
                      !use_R.y && !use_L.y && (!(ps.y > 0.0f) || !(ls.y >= lL.y && ls.y <= lR.y))};
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
         const f2 UK = sel(left, L.U(v), R.U(v));
         const f2 FK = sel(left, L.F(v), R.F(v));
-        f2 Us;
+        f2 fs;
         if (v == 1)  // E* = (E (lK - vn) + p* ls - p vn) / (lK - ls)
-            Us = mul(fma(UK, dv, sub(mul(ps, ls), mul(p, vn))), ilk);
+            fs = fma(lK, sub(mul(fma(UK, dv, sub(mul(ps, ls), mul(p, vn))), ilk), UK), FK);
         else if (v == 2 + D)  // m* = (m (lK - vn) + p* - p) / (lK - ls)
-            Us = mul(add(fma(UK, dv, ps), mul(S2(-1.0f), p)), ilk);
-        else
-            Us = mul(UK, fac);
-        const f2 fs = fma(lK, sub(Us, UK), FK);
+            fs = fma(lK, sub(mul(sub(fma(UK, dv, ps), p), ilk), UK), FK);
+        else  // U* = U fac
+            fs = fma(lkf, UK, FK);
         f2 o = sel(use_R, R.F(v), sel(use_L, L.F(v), sel(use_hll, Fh[v], fs)));
         Fo[v] = v == 1 ? mul(S2(-1.0f), o) : o;
     }
