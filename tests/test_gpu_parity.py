@@ -323,3 +323,22 @@ def test_fp32_pair_kernel_matches_scalar_kernel(rs, variant):
         e = (l1(out[name], out["fp64"], 0), l1(out[name], out["fp64"], 1))
         print(rs, variant, name, "L1 rho, p vs FP64:", e)
         assert max(e) < 1e-5
+
+
+def test_diverging_reference_newton_is_counted_as_failure():
+    """A 1D tube the reference's 1D Newton cannot follow at CFL 0.4 (from the
+    seeded batch workload): the single-grid solver keeps the reference's
+    values and counts the cells whose state became non-finite as failures."""
+    from verona_b200 import Solver
+    from verona_b200.batch import riemann_problems
+
+    specs, prims = riemann_problems(42, gamma=5.0 / 3.0)
+    sp = specs[62]
+    s = Solver(1, sp["n"], 5.0 / 3.0, (sp["dx"],), recon=sp["recon"], riemann="hllc", rk=3, n_iter=50, tol=1e-12,
+               floor=1e-8)
+    s.load_prims(prims[62])
+    s.step(sp["dt"], 10)
+    bad = int(np.sum(~np.isfinite(s.prims())))
+    c = s.counters()
+    print("non-finite values", bad, "counters", c.tolist())
+    assert bad > 0 and c[0] > 0

@@ -128,6 +128,9 @@ __global__ void __launch_bounds__(BATCH_NT) k_batch(BatchLaunch<R> a) {
         q.n_iter = a.n_iter;
         q.stats = a.stats;
         q.c2p_mode = C2P_REFERENCE;
+        q.c2p_rescue = 1;
+        q.w_rtol = 1e-12;
+        q.w_max_newton = 8;
         q.counters = a.counters;
         const bool half = a.rk == 2 && st == 0;
         q.dtdx[0] = half ? pr.dtdx[1][0] : pr.dtdx[0][0];

@@ -42,6 +42,8 @@ struct StageParams {
     int div_in_pout;     // 1: the stencil kernel left the FP32 divergence in Pout; the
                          //    con2prim kernel forms Uo = rk_a U0 + rk_b (Us - div) itself
     int want_div;        // 1: the caller's con2prim kernel (skip_c2p) accepts div_in_pout
+    int c2p_rescue;      // 1: 1D / 2D cells whose reference Newton diverges are solved by the
+                         //    bracketed W Newton (batched problems); 0: kept and counted as failures
 };
 
 template <typename R> struct StageBufs {

@@ -64,8 +64,41 @@ __device__ __forceinline__ int solve_cell(const StageParams& p, const double* U,
         fallback = fb;
         return it;
     }
-    if (DIM == 1) return c2p_1d(p.gamma, p.n_iter, p.tol, U, P);
-    if (DIM == 2) return c2p_2d(p.gamma, p.n_iter, p.tol, U, P);
+    if (DIM == 1 || DIM == 2) {
+        // the reference's 1D / 2D Newton has no failure signal: a cell that
+        // diverges keeps a non-finite state (which then spreads); it is
+        // counted here as a failure, with the reference's values kept
+        double Pin[2 + DIM];
+#pragma unroll
+        for (int v = 0; v < 2 + DIM; ++v) Pin[v] = P[v];
+        int r = DIM == 1 ? c2p_1d(p.gamma, p.n_iter, p.tol, U, P) : c2p_2d(p.gamma, p.n_iter, p.tol, U, P);
+        bool finite = true;
+#pragma unroll
+        for (int v = 0; v < 2 + DIM; ++v) finite = finite && isfinite(P[v]);
+        if (!p.c2p_rescue) return r >= 0 && finite ? r : (r < 0 ? r : -r);
+        if (r >= 0 && finite) {
+            // rescue mode also rejects a finite state that does not reproduce U
+            // (the reference's stop rule looks at the step, not the residual)
+            double Ur[2 + DIM];
+            prim2con<DIM>(p.gamma, P, Ur);
+            const double scale = fabs(U[0]) + fabs(U[1]);
+            double res = 0.0;
+#pragma unroll
+            for (int v = 0; v < 2 + DIM; ++v) res = fmax(res, fabs(Ur[v] - U[v]));
+            if (res <= 1e-8 * scale) return r;
+        }
+        // rescue (batched problems only): the bracketed W Newton from the
+        // state-only start, on the conserved state padded to three momenta;
+        // a conserved state with no physical root (no sign change of the W
+        // residual) keeps the stage's input primitive state, counted as failed
+        double U5[5] = {U[0], U[1], U[2], DIM > 1 ? U[3] : 0.0, 0.0}, P5[5];
+        int fb;
+        const int r2 = c2p_w(p.gamma, U5, U[0] - U[1], p.w_rtol, p.w_max_newton, 4 * p.n_iter, P5, &fb);
+#pragma unroll
+        for (int v = 0; v < 2 + DIM; ++v) P[v] = r2 < 0 ? Pin[v] : P5[v];
+        fallback = 1;
+        return r2;
+    }
     int r = c2p_3d(p.gamma, p.n_iter, p.tol, U, P);
     fallback = r > 1;
     return r;
