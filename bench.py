@@ -180,8 +180,9 @@ def timed_steps(s, dt, warmup, steps, dist=None):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    stage_ms, stage_launches, launches = s.profile_read()
+    stage_ms, stencil_ms, stage_launches, launches = s.profile_read2()
     s.profile(False)
+    timed_steps.stencil_ms = stencil_ms
     return ms, stage_ms, stage_launches, launches
 
 
@@ -206,6 +207,47 @@ def read_peaks():
         return float(pk["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def fp32_roofline(cells, stencil_ms, pair_stencil):
+    """Compute roofline of the FP32 stencil kernel, the binding resource of the
+    headline stage (its HBM fraction is small by construction): FP32 operations
+    per cell (2 fma + add + mul over all lanes, ncu op counters of one launch)
+    over the kernel's live CUDA-event time per launch, against SGEMM."""
+    flop = read_traffic("fp32_pairs_stencil_flop")
+    if not (pair_stencil and flop):
+        return None
+    peak = fp32_gemm_tflops()
+    ach = flop * cells / (stencil_ms / 1e3) / 1e12
+    return {"bound": "fp32", "kernel": "k_stage_zp", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+            "frac": ach / peak, "flop_per_cell": flop, "kernel_ms_per_launch": stencil_ms,
+            "peak_kind": "measured in this run: cuBLAS SGEMM 8192^3 (torch, TF32 off)"}
+
+
+def fp32_gemm_tflops():
+    """FP32 denominator of the stencil's compute roofline: cuBLAS SGEMM 8192^3
+    on the CUDA cores (TF32 off), best of 3 after one warm-up."""
+    import torch
+
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn((n, n), dtype=torch.float32, device="cuda")
+    b = torch.randn((n, n), dtype=torch.float32, device="cuda")
+    c = a @ b
+    best = None
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n**3 / (best / 1e3) / 1e12
 
 
 def fp64_gemm_tflops():
@@ -365,6 +407,7 @@ def run_ours(args, rank, world, dist):
     s.load_prims(P0)
     with Clocks(torch.cuda.current_device()) as clk:
         ms, st_ms, st_l, launches = timed_steps(s, dt, W, K, dist)
+    stencil_ms = timed_steps.stencil_ms / max(st_l, 1)
     Pf = s.store_prims()
     torch.cuda.synchronize()
     info["fast_counters"] = s.counters().tolist()
@@ -465,6 +508,8 @@ def run_ours(args, rank, world, dist):
                                 args.learned_form == "fused" else "stencil kernel + con2prim kernel(s)"),
                      "algorithmic_bytes_per_launch": bytes_per_cell_step / 3.0 * cells,
                      "stage_ms_per_launch": stage_ms_per_launch},
+        "roofline_fp32": fp32_roofline(cells, stencil_ms, learned_ok and args.learned_form == "fused"
+                                       and args.stencil == "pairs"),
         "gpu_launches": launches,
         "clocks": clk.summary,
         "e2e": e2e,

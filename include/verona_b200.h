@@ -231,6 +231,11 @@ int vb_memory_bytes(vb_handle h, uint64_t* bytes);
  * previous read, and resets them. */
 int vb_profile_enable(vb_handle h, int enable);
 int vb_profile_read(vb_handle h, double* stage_ms, int64_t* stage_launches, int64_t* all_launches);
+/* The same, with the part of the stage time spent in the stencil launcher
+ * (for the learned guess: the stencil kernel alone; otherwise the stencil
+ * and the con2prim kernel it launches). */
+int vb_profile_read2(vb_handle h, double* stage_ms, double* stencil_ms, int64_t* stage_launches,
+                     int64_t* all_launches);
 
 /* ---- point kernels: the FP64 device physics on n independent states ----------
  * Device pointers, struct-of-arrays: component k of point i at [k * n + i].

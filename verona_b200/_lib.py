@@ -94,6 +94,7 @@ _SIGS = {
     "vb_memory_bytes": [_vp, C.POINTER(C.c_uint64)],
     "vb_profile_enable": [_vp, C.c_int],
     "vb_profile_read": [_vp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
+    "vb_profile_read2": [_vp, _dp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "vb_set_tuning": [_vp, C.POINTER(VBTuning)],
     "vb_get_tuning": [_vp, C.POINTER(VBTuning)],
     "vb_point_recon": [C.c_int, _vp, _vp, C.c_int, _vp],

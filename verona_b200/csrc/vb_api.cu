@@ -484,15 +484,17 @@ int vb_init_prims(vb_handle h, const vb_ic_params* ic, void* stream) {
 
 }  // extern "C"
 
-static int prof_events(vb_handle h, cudaEvent_t* a, cudaEvent_t* b) {
-    while (h->ev.size() < h->ev_used + 2) {
+// three events per stage: start, after the stencil launcher, after the stage's con2prim
+static int prof_events(vb_handle h, cudaEvent_t* a, cudaEvent_t* m, cudaEvent_t* b) {
+    while (h->ev.size() < h->ev_used + 3) {
         cudaEvent_t e;
         VB_CUDA(h, cudaEventCreate(&e));
         h->ev.push_back(e);
     }
     *a = h->ev[h->ev_used];
-    *b = h->ev[h->ev_used + 1];
-    h->ev_used += 2;
+    *m = h->ev[h->ev_used + 1];
+    *b = h->ev[h->ev_used + 2];
+    h->ev_used += 3;
     return VB_OK;
 }
 
@@ -557,14 +559,15 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
         p.rk_a = a;
         p.rk_b = b;
         StageBufs<R> bufs{Pin, Pout, h->U0, Us, Uo};
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaEvent_t e0 = nullptr, em = nullptr, e1 = nullptr;
         if (h->prof) {
-            int rc2 = prof_events(h, &e0, &e1);
+            int rc2 = prof_events(h, &e0, &em, &e1);
             if (rc2) return rc2;
             VB_CUDA(h, cudaEventRecord(e0, s));
         }
         int nk = 0;
         VB_CUDA(h, launch_stage<R>(h->dims, h->opt.recon, h->opt.riemann, p, bufs, s, &nk));
+        if (h->prof) VB_CUDA(h, cudaEventRecord(em, s));
         if (p.skip_c2p) {
             // learned guess: the network's W per cell, then the W Newton from it
             StageParams q = p;
@@ -680,21 +683,31 @@ int vb_profile_enable(vb_handle h, int enable) {
     return VB_OK;
 }
 
-int vb_profile_read(vb_handle h, double* stage_ms, int64_t* stage_launches, int64_t* all_launches) {
-    if (!h || !stage_ms || !stage_launches || !all_launches) return fail(h, VB_ERR_ARG, "vb_profile_read: null argument");
-    double tot = 0.0;
+int vb_profile_read2(vb_handle h, double* stage_ms, double* stencil_ms, int64_t* stage_launches,
+                     int64_t* all_launches) {
+    if (!h || !stage_ms || !stencil_ms || !stage_launches || !all_launches)
+        return fail(h, VB_ERR_ARG, "vb_profile_read: null argument");
+    double tot = 0.0, sten = 0.0;
     if (h->ev_used) VB_CUDA(h, cudaEventSynchronize(h->ev[h->ev_used - 1]));
-    for (size_t i = 0; i + 1 < h->ev_used; i += 2) {
-        float ms = 0.f;
-        VB_CUDA(h, cudaEventElapsedTime(&ms, h->ev[i], h->ev[i + 1]));
+    for (size_t i = 0; i + 2 < h->ev_used; i += 3) {
+        float ms = 0.f, ms1 = 0.f;
+        VB_CUDA(h, cudaEventElapsedTime(&ms, h->ev[i], h->ev[i + 2]));
+        VB_CUDA(h, cudaEventElapsedTime(&ms1, h->ev[i], h->ev[i + 1]));
         tot += ms;
+        sten += ms1;
     }
     *stage_ms = tot;
+    *stencil_ms = sten;
     *stage_launches = h->stage_launches;
     *all_launches = h->launches;
     h->ev_used = 0;
     h->launches = h->stage_launches = 0;
     return VB_OK;
+}
+
+int vb_profile_read(vb_handle h, double* stage_ms, int64_t* stage_launches, int64_t* all_launches) {
+    double sten = 0.0;
+    return vb_profile_read2(h, stage_ms, &sten, stage_launches, all_launches);
 }
 
 int vb_attach_mlp(vb_handle h, vb_mlp_handle m) {

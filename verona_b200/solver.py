@@ -194,6 +194,12 @@ class Solver:
         L.check(L.lib().vb_profile_read(self._h, C.byref(ms), C.byref(sl), C.byref(al)), self._h)
         return ms.value, sl.value, al.value
 
+    def profile_read2(self):
+        """(stage ms, stencil-launcher ms, stage launches, all launches) since the last read."""
+        ms, st, sl, al = C.c_double(), C.c_double(), C.c_int64(), C.c_int64()
+        L.check(L.lib().vb_profile_read2(self._h, C.byref(ms), C.byref(st), C.byref(sl), C.byref(al)), self._h)
+        return ms.value, st.value, sl.value, al.value
+
     @property
     def memory_bytes(self) -> int:
         v = C.c_uint64()
