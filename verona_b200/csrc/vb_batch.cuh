@@ -25,6 +25,7 @@
 //     examples' zero-gradient TurnOff) and writes the floored copy to the
 //     stage output; later stages copy the floored ghosts of their input.
 #pragma once
+#include <type_traits>
 #include "vb_batch.h"
 #include "vb_stage.cuh"
 
@@ -127,7 +128,9 @@ __global__ void __launch_bounds__(BATCH_NT) k_batch(BatchLaunch<R> a) {
         q.tol = a.tol;
         q.n_iter = a.n_iter;
         q.stats = a.stats;
-        q.c2p_mode = C2P_REFERENCE;
+        // FP64: the reference con2prim (parity with the single-grid solver);
+        // FP32 bulk: the W Newton from the input state first (cheaper, no LU)
+        q.c2p_mode = std::is_same<R, float>::value ? C2P_GUESS_W : C2P_REFERENCE;
         q.c2p_rescue = 1;
         q.w_rtol = 1e-12;
         q.w_max_newton = 8;

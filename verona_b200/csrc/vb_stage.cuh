@@ -65,39 +65,65 @@ __device__ __forceinline__ int solve_cell(const StageParams& p, const double* U,
         return it;
     }
     if (DIM == 1 || DIM == 2) {
-        // the reference's 1D / 2D Newton has no failure signal: a cell that
-        // diverges keeps a non-finite state (which then spreads); it is
-        // counted here as a failure, with the reference's values kept
+        // The reference's 1D / 2D Newton has no failure signal: a cell that
+        // diverges keeps a non-finite state (which then spreads); without
+        // c2p_rescue (single grids) the reference's values are kept and the
+        // cell is counted as a failure. With c2p_rescue (batched problems) a
+        // reference result is accepted only if finite and reproducing U to
+        // 1e-8 (its stop rule looks at the step, not the residual), the
+        // bracketed W Newton on the conserved state padded to three momenta
+        // is the other solver, and a cell neither solves keeps the stage's
+        // input state (counted as failed). C2P_GUESS_W (FP32-bulk batches)
+        // runs the W Newton first, from the input state's W; the reference
+        // Newton, which also accepts negative-pressure roots that the floors
+        // then lift, is its fallback.
         double Pin[2 + DIM];
 #pragma unroll
         for (int v = 0; v < 2 + DIM; ++v) Pin[v] = P[v];
-        int r = DIM == 1 ? c2p_1d(p.gamma, p.n_iter, p.tol, U, P) : c2p_2d(p.gamma, p.n_iter, p.tol, U, P);
-        bool finite = true;
+        auto ref_try = [&](int& r) -> bool {
 #pragma unroll
-        for (int v = 0; v < 2 + DIM; ++v) finite = finite && isfinite(P[v]);
-        if (!p.c2p_rescue) return r >= 0 && finite ? r : (r < 0 ? r : -r);
-        if (r >= 0 && finite) {
-            // rescue mode also rejects a finite state that does not reproduce U
-            // (the reference's stop rule looks at the step, not the residual)
+            for (int v = 0; v < 2 + DIM; ++v) P[v] = Pin[v];
+            r = DIM == 1 ? c2p_1d(p.gamma, p.n_iter, p.tol, U, P) : c2p_2d(p.gamma, p.n_iter, p.tol, U, P);
+            bool finite = true;
+#pragma unroll
+            for (int v = 0; v < 2 + DIM; ++v) finite = finite && isfinite(P[v]);
+            if (!(r >= 0 && finite)) return false;
+            if (!p.c2p_rescue) return true;
             double Ur[2 + DIM];
             prim2con<DIM>(p.gamma, P, Ur);
             const double scale = fabs(U[0]) + fabs(U[1]);
             double res = 0.0;
 #pragma unroll
             for (int v = 0; v < 2 + DIM; ++v) res = fmax(res, fabs(Ur[v] - U[v]));
-            if (res <= 1e-8 * scale) return r;
-        }
-        // rescue (batched problems only): the bracketed W Newton from the
-        // state-only start, on the conserved state padded to three momenta;
-        // a conserved state with no physical root (no sign change of the W
-        // residual) keeps the stage's input primitive state, counted as failed
-        double U5[5] = {U[0], U[1], U[2], DIM > 1 ? U[3] : 0.0, 0.0}, P5[5];
-        int fb;
-        const int r2 = c2p_w(p.gamma, U5, U[0] - U[1], p.w_rtol, p.w_max_newton, 4 * p.n_iter, P5, &fb);
+            return res <= 1e-8 * scale;
+        };
+        auto w_try = [&](double W0, int& r) -> bool {
+            double U5[5] = {U[0], U[1], U[2], DIM > 1 ? U[3] : 0.0, 0.0}, P5[5];
+            int fb;
+            r = c2p_w(p.gamma, U5, W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, P5, &fb);
+            if (r < 0) return false;
 #pragma unroll
-        for (int v = 0; v < 2 + DIM; ++v) P[v] = r2 < 0 ? Pin[v] : P5[v];
-        fallback = 1;
-        return r2;
+            for (int v = 0; v < 2 + DIM; ++v) P[v] = P5[v];
+            return true;
+        };
+        int r = 0;
+        if (!p.c2p_rescue) {
+            const bool ok = ref_try(r);
+            return ok ? r : (r < 0 ? r : -(r + 1));
+        }
+        if (p.c2p_mode == C2P_GUESS_W) {
+            const double gm2 = sq(Pin[2]) + (DIM > 1 ? sq(Pin[3]) : 0.0) + 1.0;
+            if (w_try((Pin[0] + p.gamma * Pin[1]) * gm2, r)) return r;
+            fallback = 1;
+            if (ref_try(r)) return r;
+        } else {
+            if (ref_try(r)) return r;
+            fallback = 1;
+            if (w_try(U[0] - U[1], r)) return r;
+        }
+#pragma unroll
+        for (int v = 0; v < 2 + DIM; ++v) P[v] = Pin[v];
+        return r < 0 ? r : -(r + 1);
     }
     int r = c2p_3d(p.gamma, p.n_iter, p.tol, U, P);
     fallback = r > 1;
