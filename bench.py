@@ -55,6 +55,8 @@ def parse():
                     help="learned con2prim as one kernel (guess + Newton) or as a guess kernel + con2prim kernel")
     ap.add_argument("--stencil", default="pairs", choices=["pairs", "scalar"],
                     help="FP32 stencil kernel: two cells per thread on packed FP32 pairs, or one cell per thread")
+    ap.add_argument("--planes", default="tma", choices=["tma", "cp-async"],
+                    help="z-pair stencil: planes staged as TMA tiles, or by per-thread loads and cp.async halo copies")
     ap.add_argument("--dump", action="store_true",
                     help="also time an asynchronous dump of the interior (vb_dump_begin) overlapped with K steps")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -403,7 +405,8 @@ def run_ours(args, rank, world, dist):
     s = make_solver(n, "fp32", guess)
     if learned_ok:
         mlp.attach(s)
-    s.set_tuning(learned_fused=int(args.learned_form == "fused"), fp32_pairs=int(args.stencil == "pairs"))
+    s.set_tuning(learned_fused=int(args.learned_form == "fused"), fp32_pairs=int(args.stencil == "pairs"),
+                 tma_planes=int(args.planes == "tma"))
     s.load_prims(P0)
     with Clocks(torch.cuda.current_device()) as clk:
         ms, st_ms, st_l, launches = timed_steps(s, dt, W, K, dist)
@@ -496,7 +499,7 @@ def run_ours(args, rank, world, dist):
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 bulk + f64 (U, con2prim)", "data": "synthetic",
         "config": dict(workload_config(n, guess), learned_form=args.learned_form if learned_ok else None,
-                       stencil=args.stencil),
+                       stencil=args.stencil, planes=args.planes if args.stencil == "pairs" else None),
         "fp64_plain": fp64,
         "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
         "l1_error_vs_fp64": err,

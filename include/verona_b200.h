@@ -209,13 +209,19 @@ int vb_reset_counters(vb_handle h, void* stream);
  * fp32_pairs (precision = VB_PREC_FP32_BULK, 3D, WENOZ with HLL or HLLC): 1 =
  * the z-pair stencil kernel (two cells per thread on packed FP32 pairs);
  * 0 = one cell per thread; -1 = library default (1). The two agree to FP32
- * rounding, not bitwise. */
+ * rounding, not bitwise.
+ * tma_planes (z-pair stencil kernel only): 1 = every plane of the state, with
+ * its x/y halo, comes into shared memory as one TMA tile (cp.async.bulk.tensor,
+ * a ring of 6 planes per CTA); 0 = the thread loads its own column and 4-byte
+ * asynchronous copies bring the halo; -1 = library default (1). Results are
+ * identical. */
 typedef struct vb_tuning {
     int32_t split_con2prim;
     int32_t force_box;
     int32_t learned_fused;
     int32_t fp32_pairs;
-    int32_t reserved[4];
+    int32_t tma_planes;
+    int32_t reserved[3];
 } vb_tuning;
 int vb_set_tuning(vb_handle h, const vb_tuning* t);
 int vb_get_tuning(vb_handle h, vb_tuning* t);

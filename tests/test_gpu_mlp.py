@@ -193,6 +193,34 @@ def test_learned_fused_kernel_matches_two_kernel_form(net, precision):
     assert max(l1) < (1e-12 if precision == "fp64" else 2e-6)
 
 
+def test_learned_path_tma_planes_match_cp_async_planes(net):
+    """The headline form (z-pair stencil leaving the FP32 divergence, fused
+    learned con2prim) with the stencil's planes brought in as TMA tiles and
+    with per-thread loads plus asynchronous halo copies: the same values reach
+    the same arithmetic, so P and U agree bitwise."""
+    from helpers import jet_ic, nozzle_params
+    from verona_b200 import Solver
+
+    n = (64, 24, 21)
+    P0 = jet_ic(3, n, gamma=G, noise=0.03, seed=6)
+    dxs = [1.0 / 64] * 3
+    dt = 0.4 / sum(1.0 / d for d in dxs)
+    out = {}
+    for tma in (0, 1):
+        s = Solver(3, n, G, dxs, recon="wenoz", riemann="hllc", rk=3, guess="learned", precision="fp32",
+                   n_iter=50, tol=1e-12, floor=1e-8)
+        net.attach(s)
+        s.set_tuning(learned_fused=1, fp32_pairs=1, tma_planes=tma)
+        s.set_boundary(0, 2, nozzle_params(3, n, 4.0, gamma=G))
+        s.load_prims(P0)
+        s.step(dt, 4)
+        c = s.counters()
+        assert c[0] == 0 and c[4] == 0
+        out[tma] = (s.prims(), s.cons())
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
 def test_w_newton_recovers_the_primitive_state():
     """vb_point_c2p_w against the exact answer: P -> U = PtoU(P) -> P over the
     training ranges (Lorentz factor up to 40, below the solver's cap of 50),

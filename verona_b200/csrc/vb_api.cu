@@ -29,7 +29,8 @@ struct vb_solver {
     int dims = 0, nv = 0, nghost = 3;
     int n[3] = {1, 1, 1};   // interior
     int np[3] = {1, 1, 1};  // padded
-    long long ncell = 0, vs = 0;
+    long long ncell = 0, vs = 0;  // padded cells; elements between variable arrays
+    long long sy = 0, sz = 0;       // strides of j and k in the SoA arrays (rows pitched)
     vb_options opt{};
     double gamma = 5.0 / 3.0;
     double dx[3] = {1.0, 1.0, 1.0};
@@ -53,7 +54,10 @@ struct vb_solver {
     size_t bytes = 0;
     std::string err;
     // kernel variants
-    vb_tuning tun{-1, 0, -1, -1, {0, 0, 0, 0}};
+    vb_tuning tun{-1, 0, -1, -1, -1, {0, 0, 0}};
+    // TMA tensor maps of P[0], P[1] (FP32 3D; the TMA form of the z-pair kernel)
+    alignas(64) unsigned char tmap[2][128] = {};
+    bool tmap_ok[2] = {false, false};
     // learned con2prim guess
     const void* mlp_blob = nullptr;
     unsigned int* tc_err = nullptr;
@@ -98,8 +102,8 @@ static Grid grid_of(const vb_solver* h) {
     g.dims = h->dims;
     g.nv = h->nv;
     for (int a = 0; a < 3; ++a) g.n[a] = h->np[a];
-    g.sy = h->np[0];
-    g.sz = (long long)h->np[0] * h->np[1];
+    g.sy = h->sy;
+    g.sz = h->sz;
     g.vs = h->vs;
     return g;
 }
@@ -205,7 +209,11 @@ int vb_create(vb_handle* out, int dims, int nx, int ny, int nz, int nghost, cons
         h->np[a] = a < dims ? nn[a] + 2 * nghost : 1;
     }
     h->ncell = (long long)h->np[0] * h->np[1] * h->np[2];
-    h->vs = (h->ncell + 31) / 32 * 32;  // each variable array starts on a 256-byte boundary
+    // 2D / 3D rows are pitched to a multiple of 4 cells, so that every row and
+    // plane stride is a multiple of 16 bytes (the tensor-map stride rule of TMA)
+    h->sy = dims >= 2 ? (h->np[0] + 3) / 4 * 4 : h->np[0];
+    h->sz = h->sy * h->np[1];
+    h->vs = (h->sz * h->np[2] + 31) / 32 * 32;  // each variable array starts on a 256-byte boundary
     int rc;
     if (nghost == 0) {
         const int N = nx;
@@ -233,6 +241,8 @@ int vb_create(vb_handle* out, int dims, int nx, int ny, int nz, int nghost, cons
             return rc;
         }
     }
+    if (nghost != 0 && fp32(h) && dims == 3)
+        for (int i = 0; i < 2; ++i) h->tmap_ok[i] = encode_plane_tmap(h->tmap[i], (const float*)h->P[i], grid_of(h));
     h->max_partial = max_speed_blocks(grid_of(h));
     if ((rc = dev_alloc(h, (void**)&h->cnt, sizeof(unsigned long long) * CNT_N)) ||
         (rc = dev_alloc(h, (void**)&h->partial, sizeof(double) * (h->max_partial + 1)))) {
@@ -554,8 +564,12 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
         // guess kernel of the two-kernel form reads a formed U
         p.want_div = h->tun.learned_fused != 0;
     }
+    const bool tma = h->tun.tma_planes != 0;
     auto stage = [&](const R* Pin, R* Pout, const double* Us, double* Uo, double dts, double a, double b) -> int {
         for (int d = 0; d < 3; ++d) p.dtdx[d] = d < h->dims ? dts / h->dx[d] : 0.0;
+        p.tmap_in = nullptr;
+        for (int i = 0; i < 2; ++i)
+            if (tma && h->tmap_ok[i] && (const void*)Pin == h->P[i]) p.tmap_in = h->tmap[i];
         p.rk_a = a;
         p.rk_b = b;
         StageBufs<R> bufs{Pin, Pout, h->U0, Us, Uo};
@@ -729,10 +743,11 @@ int vb_attach_mlp(vb_handle h, vb_mlp_handle m) {
 int vb_set_tuning(vb_handle h, const vb_tuning* t) {
     if (!h || !t) return fail(h, VB_ERR_ARG, "vb_set_tuning: null argument");
     if (t->split_con2prim < -1 || t->split_con2prim > 1 || t->force_box < 0 || t->force_box > 1 ||
-        t->learned_fused < -1 || t->learned_fused > 1 || t->fp32_pairs < -1 || t->fp32_pairs > 1)
+        t->learned_fused < -1 || t->learned_fused > 1 || t->fp32_pairs < -1 || t->fp32_pairs > 1 ||
+        t->tma_planes < -1 || t->tma_planes > 1)
         return fail(h, VB_ERR_ARG,
-                    "vb_set_tuning: split_con2prim in {-1,0,1}, force_box in {0,1}, learned_fused and fp32_pairs "
-                    "in {-1,0,1}");
+                    "vb_set_tuning: split_con2prim in {-1,0,1}, force_box in {0,1}, learned_fused, fp32_pairs and "
+                    "tma_planes in {-1,0,1}");
     h->tun = *t;
     return VB_OK;
 }

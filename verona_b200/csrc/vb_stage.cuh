@@ -374,6 +374,14 @@ cudaError_t launch_stage(int dims, int rec, int rs, const StageParams& p, const 
 // ---- layout conversion -----------------------------------------------------
 // One thread per cell; AoS reads of nv consecutive doubles, SoA writes are
 // coalesced per variable.
+
+// dense padded cell c (x fastest, rows of n[0] cells) -> index in the pitched SoA arrays
+__device__ __forceinline__ long long soa_index(const Grid& g, long long c) {
+    if (g.sy == g.n[0]) return c;
+    const long long row = c / g.n[0];
+    return (c - row * g.n[0]) + g.sy * row;  // sz == sy * n[1]: rows of every plane are consecutive
+}
+
 template <int DIM, typename R>
 __global__ void k_load_prims(Grid g, const double* __restrict__ Pa, R* __restrict__ P, double* __restrict__ U0,
                              double gamma) {
@@ -385,10 +393,11 @@ __global__ void k_load_prims(Grid g, const double* __restrict__ Pa, R* __restric
 #pragma unroll
         for (int v = 0; v < NV; ++v) q[v] = Pa[c * NV + v];
         prim2con<DIM>(gamma, q, u);  // kernel_PtoU, src/3dim/structs.jl:66-81
+        const long long s = soa_index(g, c);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            P[v * g.vs + c] = (R)q[v];
-            U0[v * g.vs + c] = u[v];
+            P[v * g.vs + s] = (R)q[v];
+            U0[v * g.vs + s] = u[v];
         }
     }
 }
@@ -399,8 +408,9 @@ __global__ void k_store_prims(Grid g, const R* __restrict__ P, double* __restric
     long long ncell = (long long)g.n[0] * g.n[1] * g.n[2];
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
          c += (long long)gridDim.x * blockDim.x) {
+        const long long s = soa_index(g, c);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Pa[c * NV + v] = (double)P[v * g.vs + c];
+        for (int v = 0; v < NV; ++v) Pa[c * NV + v] = (double)P[v * g.vs + s];
     }
 }
 
@@ -469,10 +479,11 @@ __global__ void k_init_prims(Grid g, InitIC ic, R* __restrict__ P, double* __res
         }
         double uc[NV];
         prim2con<DIM>(gamma, q, uc);
+        const long long s = soa_index(g, c);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            P[v * g.vs + c] = (R)q[v];
-            U0[v * g.vs + c] = uc[v];
+            P[v * g.vs + s] = (R)q[v];
+            U0[v * g.vs + s] = uc[v];
         }
     }
 }

@@ -16,7 +16,10 @@
 // FP64 exactly as in k_stage_zm. Same scheme as the reference's 3D kernels
 // (src/3dim/algos.jl:14-200, src/fluxlimiter.jl:19-71) plus HLLC.
 #pragma once
+#include <cuda.h>  // CUtensorMap
+
 #include "vb_stage_zm.cuh"
+#include "vb_tc.cuh"
 
 namespace vb {
 namespace pk {
@@ -240,23 +243,63 @@ template <int TX, int TY> struct ZpGeom {
     }
 };
 
+// Ring of the TMA form: plane z of every variable, with its x/y halo, in slot
+// z % ZR as one TMA box [NV][EY][BXW] (x fastest). The box starts at
+// x = i0 - 3 = TX * blockIdx.x, a multiple of 4 cells (16 bytes, the TMA
+// coordinate rule), and is BXW >= TX + 6 cells wide, a multiple of 4.
+template <int TX, int TY> struct ZpTmaGeom {
+    static constexpr int NV = 5, ZR = 6;
+    static constexpr int BXW = (TX + 6 + 3) / 4 * 4, EY = TY + 6;
+    static constexpr int VSTR = EY * BXW;                        // floats between variables in a slot
+    static constexpr int BOX_BYTES = 4 * NV * VSTR;              // one plane, every variable
+    static constexpr int SLOTF = (BOX_BYTES + 127) / 128 * 128 / 4;  // floats per slot (128-byte aligned)
+    static constexpr size_t smem_bytes() {
+        using G = ZpGeom<TX, TY>;
+        return 128 + 4 * (size_t)ZR * SLOTF + sizeof(float2) * NV * (size_t)(2 * G::FN + G::QXN) + 8 * ZR;
+    }
+};
+constexpr uint32_t ZP_MAX_POLLS = 1u << 22;  // bounded waits for a TMA plane
+
 // What a pair stage kernel leaves behind: con2prim done in the kernel (fused),
 // U for k_c2p (split), or the FP32 divergence in Pout for the learned
 // con2prim kernel, which forms U itself (div).
 enum { ZP_FUSED = 0, ZP_U = 1, ZP_DIV = 2 };
 
-template <int RS, int TX, int TY, int LZ, int MINB, int TAIL>
-__global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, StageBufs<float> b) {
+// TMA: the planes come as TMA boxes into a ring of ZR slots (ZpTmaGeom, tm:
+// the tensor map of Pin, dims (x, y, z, variable)); otherwise the column's
+// z-window is loaded by the thread and the x/y halo of the planes (k, k+1)
+// by 4-byte asynchronous copies into an interleaved pair buffer.
+template <int RS, int TX, int TY, int LZ, int MINB, int TAIL, bool TMA>
+__global__ void __launch_bounds__(TX * TY, MINB)
+    k_stage_zp(StageParams p, StageBufs<float> b, const __grid_constant__ CUtensorMap tm) {
     using namespace pk;
     using G = ZpGeom<TX, TY>;
-    constexpr int NV = 5, NT = G::NT, EX = G::EX, PLN = G::PLN, FN = G::FN, QXN = G::QXN, ZR = G::ZR;
+    using TG = ZpTmaGeom<TX, TY>;
+    constexpr int NV = 5, NT = G::NT, FN = G::FN, QXN = G::QXN, ZR = G::ZR;
     constexpr int FXR = TX + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    f2* sPl = reinterpret_cast<f2*>(smem_raw);  // [NV][EY][EX]: planes (k, k+1) with x/y halo
-    f2* sQL = sPl + NV * PLN;                     // [NV][FN]: left states of the faces
-    f2* sF = sQL + NV * FN;                       // [NV][FN]: face fluxes
-    f2* sQX = sF + NV * FN;                       // [NV][QXN]: right states of the last faces
-    float* sZ = reinterpret_cast<float*>(sQX + NV * QXN);  // [ZR][NV][NT]: this thread's z-window
+    // plane access: element (v, y, x) of a plane at v * VSTR + (y + 3) * ROW + x + 3
+    constexpr int ROW = TMA ? TG::BXW : G::EX, VSTR = TMA ? TG::VSTR : G::PLN, SLOTF = TG::SLOTF;
+    static_assert(!TMA || TX % 4 == 0, "TMA boxes start at x = TX * blockIdx.x");
+    extern __shared__ __align__(16) unsigned char smem_raw[];  // TMA form: 128-byte base found below
+    f2* sPl = nullptr;         // cp.async form: [NV][EY][EX] planes (k, k+1) with x/y halo
+    float* sZ = nullptr;       // cp.async form: [ZR][NV][NT] this thread's z-window
+    float* sRing = nullptr;    // TMA form: [ZR][SLOTF] plane boxes
+    uint64_t* sBar = nullptr;  // TMA form: one mbarrier per ring slot
+    f2 *sQL, *sF, *sQX;        // [NV][FN] left states, [NV][FN] fluxes, [NV][QXN] last right states
+    if constexpr (TMA) {
+        unsigned char* base = smem_raw + ((128u - (tc::smem_u32(smem_raw) & 127u)) & 127u);
+        sRing = reinterpret_cast<float*>(base);
+        sQL = reinterpret_cast<f2*>(sRing + ZR * SLOTF);
+        sF = sQL + NV * FN;
+        sQX = sF + NV * FN;
+        sBar = reinterpret_cast<uint64_t*>(sQX + NV * QXN);
+    } else {
+        sPl = reinterpret_cast<f2*>(smem_raw);
+        sQL = sPl + NV * G::PLN;
+        sF = sQL + NV * FN;
+        sQX = sF + NV * FN;
+        sZ = reinterpret_cast<float*>(sQX + NV * QXN);
+    }
 
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
@@ -270,7 +313,12 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
     const f2 g = S2((float)p.gamma), gm1 = S2((float)(p.gamma - 1.0));
     const f2 cx = S2((float)p.dtdx[0]), cy = S2((float)p.dtdx[1]), cz = S2((float)p.dtdx[2]);
 
-    auto zs = [&](int z, int v) -> float& { return sZ[((z % ZR) * NV + v) * NT + tid]; };
+    auto zs = [&](int z, int v) -> float& {
+        if constexpr (TMA)
+            return sRing[(z % ZR) * SLOTF + v * VSTR + (ty + 3) * ROW + tx + 3];
+        else
+            return sZ[((z % ZR) * NV + v) * NT + tid];
+    };
     auto zload = [&](int z) {
         const bool in = z < p.n[2];
 #pragma unroll
@@ -309,18 +357,42 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
             const long long gc = (i0 + hx) + sy * (j0 + hy) + sz * kk;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                f2* d = &sPl[v * PLN + (hy + 3) * EX + hx + 3];
+                f2* d = &sPl[v * VSTR + (hy + 3) * ROW + hx + 3];
                 cp_async4(&d->x, b.Pin + v * vs + gc);
                 cp_async4(&d->y, b.Pin + v * vs + gc + sz);
             }
         }
     };
-    halo_issue(z0);
+    // TMA form: plane z -> slot z % ZR (one thread issues); plane z is the
+    // ((z - z0 + 3) / ZR)-th load of its slot, which fixes the phase parity
+    auto plane_issue = [&](int z) {
+        uint64_t* bar = &sBar[z % ZR];
+        tc::mbar_arrive_expect_tx(bar, TG::BOX_BYTES);
+        tc::tma_load_4d(sRing + (z % ZR) * SLOTF, &tm, i0 - NG, j0 - NG, z, 0, bar);
+    };
+    auto plane_wait = [&](int z) -> bool {
+        const uint32_t parity = (uint32_t)((z - z0 + NG) / ZR) & 1u;
+        return tc::mbar_wait(&sBar[z % ZR], parity, nullptr, ZP_MAX_POLLS);
+    };
+    bool stalled = false;  // TMA form: a plane wait ran out (uniform after the next barrier)
+    int z_issued = z0 + 2;  // TMA form: last plane issued
 
     float qlz[NV];  // ql of cell k (left state of face k+1/2)
     float Fzm[NV];  // flux at face k-1/2
     // prologue: window z0-3 .. z0+2, cells (z0-1, z0), the flux at z0-1/2 (both lanes), then z0+3, z0+4
-    for (int z = z0 - 3; z <= z0 + 2; ++z) zload(z);
+    if constexpr (TMA) {
+        if (tid == 0) {
+            for (int s = 0; s < ZR; ++s) tc::mbar_init(&sBar[s], 1);
+            tc::fence_mbar_init();
+        }
+        __syncthreads();
+        if (tid == 0)
+            for (int z = z0 - 3; z <= z0 + 2; ++z) plane_issue(z);
+        for (int z = z0 - 3; z <= z0 + 2; ++z) stalled |= !plane_wait(z);
+    } else {
+        halo_issue(z0);
+        for (int z = z0 - 3; z <= z0 + 2; ++z) zload(z);
+    }
     {
         f2 qr[NV], ql[NV], L[NV], R[NV], F[NV];
         zrecon(z0 - 1, qr, ql);
@@ -334,8 +406,10 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
 #pragma unroll
         for (int v = 0; v < NV; ++v) Fzm[v] = F[v].x;
     }
-    zload(z0 + 3);
-    zload(z0 + 4);
+    if constexpr (!TMA) {
+        zload(z0 + 3);
+        zload(z0 + 4);
+    }
 
     unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
     for (int k = z0; k < zend; k += 2) {
@@ -346,21 +420,43 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
         for (int v = 0; v < NV; ++v) acc[v] = S2(0.0f);
 
         // stage planes (k, k+1): own column from the window; the halo copies were
-        // issued earlier (plane k+1 <= zend <= n2 - 3 exists even when the pair is incomplete)
+        // issued earlier (plane k+1 <= zend <= n2 - 3 exists even when the pair is incomplete).
+        // TMA form: planes k, k+1 are in the ring (waited for by the previous z step);
+        // once every thread is past the previous step, planes k+3, k+4 replace k-3, k-2
+        if constexpr (TMA) {
+            if (__syncthreads_or(stalled)) {
+                stalled = true;
+                break;
+            }
+            if (tid == 0) {
+                tc::fence_proxy_async();
+                plane_issue(k + 3);
+                plane_issue(k + 4);
+            }
+            z_issued = k + 4;
+        } else {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) sPl[v * PLN + (ty + 3) * EX + tx + 3] = P2(zs(k, v), zs(k + 1, v));
-        cp_async_wait_all();
-        __syncthreads();
+            for (int v = 0; v < NV; ++v) sPl[v * VSTR + (ty + 3) * ROW + tx + 3] = P2(zs(k, v), zs(k + 1, v));
+            cp_async_wait_all();
+            __syncthreads();
+        }
+        // pair of planes (k, k+1) at offset o of a variable's plane
+        const int sk = (k % ZR) * SLOTF, sk1 = ((k + 1) % ZR) * SLOTF;
+        auto pq = [&](int v, int o) -> f2 {
+            if constexpr (TMA)
+                return P2(sRing[sk + v * VSTR + o], sRing[sk1 + v * VSTR + o]);
+            else
+                return sPl[v * VSTR + o];
+        };
 
         // x: reconstruct own cells; halo cells -1 and TX of each row
         f2 qrx[NV];
         {
-            const f2* q = sPl + (ty + 3) * EX + tx + 3;
+            const int o = (ty + 3) * ROW + tx + 3;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                const f2* qv = q + v * PLN;
                 f2 qr, ql;
-                wenoz(qv[-2], qv[-1], qv[0], qv[1], qv[2], qr, ql);
+                wenoz(pq(v, o - 2), pq(v, o - 1), pq(v, o), pq(v, o + 1), pq(v, o + 2), qr, ql);
                 if (v < 2) {
                     qr = vmax(fl, qr);
                     ql = vmax(fl, ql);
@@ -377,9 +473,9 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
             const int lane = tid & 31, e = (tid >> 5) * XPW + lane;
             if (lane < XPW && e < XH) {
                 const int v = e % NV, cell = e / NV, r = cell >> 1, side = cell & 1;
-                const f2* qv = sPl + v * PLN + (r + 3) * EX + (side ? TX : -1) + 3;
+                const int o = (r + 3) * ROW + (side ? TX : -1) + 3;
                 f2 qr, ql;
-                wenoz(qv[-2], qv[-1], qv[0], qv[1], qv[2], qr, ql);
+                wenoz(pq(v, o - 2), pq(v, o - 1), pq(v, o), pq(v, o + 1), pq(v, o + 2), qr, ql);
                 if (v < 2) {
                     qr = vmax(fl, qr);
                     ql = vmax(fl, ql);
@@ -418,12 +514,11 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
         // y: reconstruct own cells; halo cells -1 and TY of each column
         f2 qry[NV];
         {
-            const f2* q = sPl + (ty + 3) * EX + tx + 3;
+            const int o = (ty + 3) * ROW + tx + 3;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                const f2* qv = q + v * PLN;
                 f2 qr, ql;
-                wenoz(qv[-2 * EX], qv[-EX], qv[0], qv[EX], qv[2 * EX], qr, ql);
+                wenoz(pq(v, o - 2 * ROW), pq(v, o - ROW), pq(v, o), pq(v, o + ROW), pq(v, o + 2 * ROW), qr, ql);
                 if (v < 2) {
                     qr = vmax(fl, qr);
                     ql = vmax(fl, ql);
@@ -435,9 +530,9 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
         // halo cells -1 and TY of every column, one (cell, variable) per thread
         for (int e = tid; e < 2 * TX * NV; e += NT) {
             const int v = e / (2 * TX), cell = e % (2 * TX), cx_ = cell % TX, side = cell / TX;
-            const f2* qv = sPl + v * PLN + ((side ? TY : -1) + 3) * EX + cx_ + 3;
+            const int o = ((side ? TY : -1) + 3) * ROW + cx_ + 3;
             f2 qr, ql;
-            wenoz(qv[-2 * EX], qv[-EX], qv[0], qv[EX], qv[2 * EX], qr, ql);
+            wenoz(pq(v, o - 2 * ROW), pq(v, o - ROW), pq(v, o), pq(v, o + ROW), pq(v, o + 2 * ROW), qr, ql);
             if (v < 2) {
                 qr = vmax(fl, qr);
                 ql = vmax(fl, ql);
@@ -449,7 +544,9 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
         }
         __syncthreads();
         // every read of sPl for this pair is done: fetch the next pair's halo
-        if (k + 2 < zend) halo_issue(k + 2);
+        if constexpr (!TMA) {
+            if (k + 2 < zend) halo_issue(k + 2);
+        }
         {
             f2 PL[NV], F[NV];
 #pragma unroll
@@ -477,12 +574,18 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
         // z: planes k+5, k+6 are fetched now and enter the window after the
         // reconstruction of cells (k+1, k+2) from planes k-1 .. k+4; faces
         // k+1/2 (left ql(k), right qr(k+1)) and k+3/2 (left ql(k+1), right qr(k+2))
+        // (TMA form: planes k+3, k+4 were issued at the top of this step)
         float nxt[2 * NV];
+        if constexpr (TMA) {
+            stalled |= !plane_wait(k + 3);
+            stalled |= !plane_wait(k + 4);
+        } else {
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const bool in = k + 5 + q < p.n[2];
+            for (int q = 0; q < 2; ++q) {
+                const bool in = k + 5 + q < p.n[2];
 #pragma unroll
-            for (int v = 0; v < NV; ++v) nxt[q * NV + v] = in ? b.Pin[v * vs + c + (5 + q) * sz] : 0.0f;
+                for (int v = 0; v < NV; ++v) nxt[q * NV + v] = in ? b.Pin[v * vs + c + (5 + q) * sz] : 0.0f;
+            }
         }
         float Pk[2 * NV];
 #pragma unroll
@@ -503,10 +606,12 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
                 qlz[v] = ql1[v].y;
             }
         }
+        if constexpr (!TMA) {
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < 2; ++q)
 #pragma unroll
-            for (int v = 0; v < NV; ++v) zs(k + 5 + q, v) = nxt[q * NV + v];
+                for (int v = 0; v < NV; ++v) zs(k + 5 + q, v) = nxt[q * NV + v];
+        }
 
         // ZP_DIV: the FP32 divergence into Pout; ZP_U: the RK combination in FP64
         // (U - div) into Uo; ZP_FUSED: that, then con2prim (guess: this stage's P)
@@ -548,6 +653,15 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zp(StageParams p, Stage
         }
     }
 
+    if constexpr (TMA) {
+        // the loop waited for every plane it issued unless a wait ran out: then
+        // wait (bounded) for the newest load of each slot before the CTA exits
+        if (__syncthreads_or(stalled)) {
+            for (int z = z_issued - ZR + 1; z <= z_issued; ++z)
+                if (z >= z0 - NG) plane_wait(z);
+            if (tid == 0) count_add(p.counters, CNT_TIMEOUT, 1);
+        }
+    }
     if (n_fail) count_add(p.counters, CNT_C2P_FAIL, n_fail);
     if (p.stats) {
         for (int o = 16; o > 0; o >>= 1) {
@@ -571,12 +685,11 @@ struct ZpCfg {
     static constexpr int TX = 32, TY = 8, LZ = 64, MINB = 2, MINB_SPLIT = 2;
 };
 
-template <int RS, int TAIL>
+template <int RS, int TAIL, bool TMA>
 cudaError_t launch_stage_zp_t(const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
     using C = ZpCfg;
-    using G = ZpGeom<C::TX, C::TY>;
-    auto kern = k_stage_zp<RS, C::TX, C::TY, C::LZ, TAIL == ZP_FUSED ? C::MINB : C::MINB_SPLIT, TAIL>;
-    constexpr size_t smem = G::smem_bytes();
+    auto kern = k_stage_zp<RS, C::TX, C::TY, C::LZ, TAIL == ZP_FUSED ? C::MINB : C::MINB_SPLIT, TAIL, TMA>;
+    constexpr size_t smem = TMA ? ZpTmaGeom<C::TX, C::TY>::smem_bytes() : ZpGeom<C::TX, C::TY>::smem_bytes();
     static unsigned long long attr_set = 0;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -588,7 +701,12 @@ cudaError_t launch_stage_zp_t(const StageParams& p, const StageBufs<float>& b, c
         attr_set |= 1ULL << (dev & 63);
     }
     dim3 grid((p.n[0] - 2 * NG) / C::TX, (p.n[1] - 2 * NG) / C::TY, (p.n[2] - 2 * NG + C::LZ - 1) / C::LZ);
-    kern<<<grid, C::TX * C::TY, smem, s>>>(p, b);
+    CUtensorMap tm;
+    if (TMA)
+        tm = *static_cast<const CUtensorMap*>(p.tmap_in);
+    else
+        memset(&tm, 0, sizeof tm);
+    kern<<<grid, C::TX * C::TY, smem, s>>>(p, b, tm);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || TAIL != ZP_U || p.skip_c2p) return e;
     const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
@@ -602,10 +720,15 @@ cudaError_t launch_stage_zp_t(const StageParams& p, const StageBufs<float>& b, c
 // (p.want_div, the fused learned kernel), which saves the stencil kernel every
 // FP64 load and store; the reference con2prim cascade of k_c2p, bound by its
 // own memory latency, keeps reading a formed U (ZP_U).
+template <int RS, bool TMA>
+cudaError_t dispatch_stage_zp_tail(const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
+    if (!(p.split || p.skip_c2p)) return launch_stage_zp_t<RS, ZP_FUSED, TMA>(p, b, s);
+    if (p.skip_c2p && p.want_div) return launch_stage_zp_t<RS, ZP_DIV, TMA>(p, b, s);
+    return launch_stage_zp_t<RS, ZP_U, TMA>(p, b, s);
+}
+// the TMA form where the caller encoded a tensor map of Pin (p.tmap_in)
 template <int RS> cudaError_t dispatch_stage_zp_rs(const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
-    if (!(p.split || p.skip_c2p)) return launch_stage_zp_t<RS, ZP_FUSED>(p, b, s);
-    if (p.skip_c2p && p.want_div) return launch_stage_zp_t<RS, ZP_DIV>(p, b, s);
-    return launch_stage_zp_t<RS, ZP_U>(p, b, s);
+    return p.tmap_in ? dispatch_stage_zp_tail<RS, true>(p, b, s) : dispatch_stage_zp_tail<RS, false>(p, b, s);
 }
 inline cudaError_t dispatch_stage_zp(int rs, const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
     return rs == RS_HLLC ? dispatch_stage_zp_rs<RS_HLLC>(p, b, s) : dispatch_stage_zp_rs<RS_HLL>(p, b, s);

@@ -94,6 +94,30 @@ __device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
 }
 
+// make the mbarrier initialisations of this thread visible to the async proxy (TMA, tcgen05)
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// arrive once on an mbarrier and expect `bytes` more of asynchronous copies in this phase
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+                 : "memory");
+}
+
+// TMA tiled load of one box of a 4D tensor map (no multicast): the box at
+// element coordinates (c0 innermost .. c3) -> shared memory at dst (128-byte
+// aligned), completion counted in bytes on mbar. Elements outside the tensor
+// read as zero. c0 * element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, int c0, int c1, int c2, int c3,
+                                            uint64_t* mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(mbar))
+        : "memory");
+}
+
 // bounded wait for phase `parity` of an mbarrier; false (and *err set) on timeout
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, unsigned int* err, uint32_t max_polls) {
     const uint32_t a = smem_u32(mbar);
