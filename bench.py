@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--dump", action="store_true",
                     help="also time an asynchronous dump of the interior (vb_dump_begin) overlapped with K steps")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", default="jet3d", choices=["jet3d", "batch"],
+    ap.add_argument("--workload", default="jet3d", choices=["jet3d", "batch", "jet2d"],
                     help="batch: 256 uneven 1D/2D Riemann problems in one persistent launch (not the headline)")
     return ap.parse_args()
 
@@ -406,7 +406,7 @@ def run_ours(args, rank, world, dist):
     if learned_ok:
         mlp.attach(s)
     s.set_tuning(learned_fused=int(args.learned_form == "fused"), fp32_pairs=int(args.stencil == "pairs"),
-                 tma_planes=int(args.planes == "tma"))
+                 tma_tiles=int(args.planes == "tma"))
     s.load_prims(P0)
     with Clocks(torch.cuda.current_device()) as clk:
         ms, st_ms, st_l, launches = timed_steps(s, dt, W, K, dist)
@@ -641,6 +641,57 @@ def run_batch(args, rank, world, dist):
     print(json.dumps(line), flush=True)
 
 
+def run_jet2d(args, rank, world, dist):
+    """2D relativistic jet 4096^2 (n x n with --n above 512), WENOZ + HLLC,
+    SSP-RK3, CFL 0.4, gamma 4/3: ambient rho = 1 (3 % seeded noise), p = 1e-3,
+    v = 0; nozzle of radius 32 cells on the x-lo face (rho 0.01, p 1e-3,
+    Lorentz factor 10 along +x), outflow elsewhere. FP64 (the plain method) and
+    the FP32-bulk form, each timed over K steps on the device; value = the
+    FP64 form's zone-updates/s summed over ranks (independent replicas)."""
+    import math
+
+    import torch
+
+    from verona_b200 import Solver
+
+    n = args.n if args.n > 512 else 4096
+    K, W = args.steps, args.warmup
+    dx = 1.0 / n
+    dt = 0.4 / (2.0 * n)
+    tma = int(args.planes == "tma")
+    res = {}
+    with Clocks(torch.cuda.current_device()) as clk:
+        for prec in ("fp64", "fp32"):
+            s = Solver(2, (n, n), GAMMA, (dx, dx), recon="wenoz", riemann="hllc", rk=3, precision=prec, n_iter=50,
+                       tol=1e-12, floor=1e-8)
+            s.set_tuning(tma_tiles=tma)
+            s.set_boundary(0, 2, [32.0, n / 2, 0.0, 0.01, 1e-3 / (GAMMA - 1), math.sqrt(99.0), 0.0, 0.0])
+            s.init_prims("ambient", seed=7 + rank, noise=0.03, rho=1.0, u=1e-3 / (GAMMA - 1))
+            ms, st_ms, st_l, launches = timed_steps(s, dt, W, K, dist)
+            t = torch.tensor([ms], device="cuda")
+            if dist is not None:
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            c = s.counters()
+            res[prec] = {"value": world * n * n * K / (t.item() / 1e3), "ms_per_step": t.item() / K,
+                         "stage_ms_per_launch": st_ms / max(st_l, 1), "c2p_failures": int(c[0]),
+                         "tma_timeouts": int(c[4])}
+            del s
+    if rank != 0:
+        return
+    line = {
+        "metric": "zone-updates/s on 1 B200, 2D jet (plain FP64 method)", "value": res["fp64"]["value"],
+        "unit": "zone-updates/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": res["fp64"]["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"2D relativistic jet {n}^2, WENOZ+HLLC, SSP-RK3, CFL 0.4, gamma 4/3, nozzle r=32 "
+                               "Gamma=10", "grid": [n, n], "tiles": args.planes,
+                   "l2": "inputs larger than L2" if n * n * 4 * 8 > 126e6 else "inputs smaller than L2",
+                   "parallelism": "replicas"},
+        "fp64": res["fp64"], "fp32_bulk": res["fp32"], "clocks": clk.summary,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -663,6 +714,8 @@ def main():
     try:
         if args.workload == "batch":
             run_batch(args, rank, world, dist)
+        elif args.workload == "jet2d":
+            run_jet2d(args, rank, world, dist)
         else:
             run_ours(args, rank, world, dist)
     finally:

@@ -210,17 +210,18 @@ int vb_reset_counters(vb_handle h, void* stream);
  * the z-pair stencil kernel (two cells per thread on packed FP32 pairs);
  * 0 = one cell per thread; -1 = library default (1). The two agree to FP32
  * rounding, not bitwise.
- * tma_planes (z-pair stencil kernel only): 1 = every plane of the state, with
- * its x/y halo, comes into shared memory as one TMA tile (cp.async.bulk.tensor,
- * a ring of 6 planes per CTA); 0 = the thread loads its own column and 4-byte
- * asynchronous copies bring the halo; -1 = library default (1). Results are
- * identical. */
+ * tma_tiles: 1 = the stencil kernels stage the state in shared memory as TMA
+ * tiles (cp.async.bulk.tensor): in 3D (FP32 bulk, z-pair kernel) every plane
+ * with its x/y halo, a ring of 6 planes per CTA; in 2D (both precisions) the
+ * CTA's tile with its halo on both axes; 0 = staged by per-thread loads (3D:
+ * the thread's own column, 4-byte asynchronous copies for the halo);
+ * -1 = library default (1). Results are identical. */
 typedef struct vb_tuning {
     int32_t split_con2prim;
     int32_t force_box;
     int32_t learned_fused;
     int32_t fp32_pairs;
-    int32_t tma_planes;
+    int32_t tma_tiles;
     int32_t reserved[3];
 } vb_tuning;
 int vb_set_tuning(vb_handle h, const vb_tuning* t);

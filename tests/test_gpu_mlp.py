@@ -193,7 +193,7 @@ def test_learned_fused_kernel_matches_two_kernel_form(net, precision):
     assert max(l1) < (1e-12 if precision == "fp64" else 2e-6)
 
 
-def test_learned_path_tma_planes_match_cp_async_planes(net):
+def test_learned_path_tma_tiles_match_cp_async_planes(net):
     """The headline form (z-pair stencil leaving the FP32 divergence, fused
     learned con2prim) with the stencil's planes brought in as TMA tiles and
     with per-thread loads plus asynchronous halo copies: the same values reach
@@ -210,7 +210,7 @@ def test_learned_path_tma_planes_match_cp_async_planes(net):
         s = Solver(3, n, G, dxs, recon="wenoz", riemann="hllc", rk=3, guess="learned", precision="fp32",
                    n_iter=50, tol=1e-12, floor=1e-8)
         net.attach(s)
-        s.set_tuning(learned_fused=1, fp32_pairs=1, tma_planes=tma)
+        s.set_tuning(learned_fused=1, fp32_pairs=1, tma_tiles=tma)
         s.set_boundary(0, 2, nozzle_params(3, n, 4.0, gamma=G))
         s.load_prims(P0)
         s.step(dt, 4)

@@ -55,7 +55,7 @@ struct vb_solver {
     std::string err;
     // kernel variants
     vb_tuning tun{-1, 0, -1, -1, -1, {0, 0, 0}};
-    // TMA tensor maps of P[0], P[1] (FP32 3D; the TMA form of the z-pair kernel)
+    // TMA tensor maps of P[0], P[1] (the TMA forms of the stage kernels: 3D FP32, 2D)
     alignas(64) unsigned char tmap[2][128] = {};
     bool tmap_ok[2] = {false, false};
     // learned con2prim guess
@@ -241,8 +241,10 @@ int vb_create(vb_handle* out, int dims, int nx, int ny, int nz, int nghost, cons
             return rc;
         }
     }
-    if (nghost != 0 && fp32(h) && dims == 3)
-        for (int i = 0; i < 2; ++i) h->tmap_ok[i] = encode_plane_tmap(h->tmap[i], (const float*)h->P[i], grid_of(h));
+    if (nghost != 0 && dims >= 2)
+        for (int i = 0; i < 2; ++i)
+            h->tmap_ok[i] = fp32(h) ? encode_stage_tmap<float>(h->tmap[i], (const float*)h->P[i], grid_of(h))
+                                    : encode_stage_tmap<double>(h->tmap[i], (const double*)h->P[i], grid_of(h));
     h->max_partial = max_speed_blocks(grid_of(h));
     if ((rc = dev_alloc(h, (void**)&h->cnt, sizeof(unsigned long long) * CNT_N)) ||
         (rc = dev_alloc(h, (void**)&h->partial, sizeof(double) * (h->max_partial + 1)))) {
@@ -564,7 +566,7 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
         // guess kernel of the two-kernel form reads a formed U
         p.want_div = h->tun.learned_fused != 0;
     }
-    const bool tma = h->tun.tma_planes != 0;
+    const bool tma = h->tun.tma_tiles != 0;
     auto stage = [&](const R* Pin, R* Pout, const double* Us, double* Uo, double dts, double a, double b) -> int {
         for (int d = 0; d < 3; ++d) p.dtdx[d] = d < h->dims ? dts / h->dx[d] : 0.0;
         p.tmap_in = nullptr;
@@ -744,10 +746,10 @@ int vb_set_tuning(vb_handle h, const vb_tuning* t) {
     if (!h || !t) return fail(h, VB_ERR_ARG, "vb_set_tuning: null argument");
     if (t->split_con2prim < -1 || t->split_con2prim > 1 || t->force_box < 0 || t->force_box > 1 ||
         t->learned_fused < -1 || t->learned_fused > 1 || t->fp32_pairs < -1 || t->fp32_pairs > 1 ||
-        t->tma_planes < -1 || t->tma_planes > 1)
+        t->tma_tiles < -1 || t->tma_tiles > 1)
         return fail(h, VB_ERR_ARG,
                     "vb_set_tuning: split_con2prim in {-1,0,1}, force_box in {0,1}, learned_fused, fp32_pairs and "
-                    "tma_planes in {-1,0,1}");
+                    "tma_tiles in {-1,0,1}");
     h->tun = *t;
     return VB_OK;
 }

@@ -44,8 +44,8 @@ struct StageParams {
     int want_div;        // 1: the caller's con2prim kernel (skip_c2p) accepts div_in_pout
     int c2p_rescue;      // 1: 1D / 2D cells whose reference Newton diverges are solved by the
                          //    bracketed W Newton (batched problems); 0: kept and counted as failures
-    const void* tmap_in; // host CUtensorMap of Pin (dims x, y, z, variable; FP32) for the TMA form
-                         //    of the z-pair kernel; nullptr: the cp.async form
+    const void* tmap_in; // host CUtensorMap of Pin (encode_stage_tmap) for the TMA forms: the 3D
+                         //    z-pair kernel's planes, k_stage's 2D tiles; nullptr: staged by loads
 };
 
 template <typename R> struct StageBufs {
@@ -117,9 +117,11 @@ int max_speed_blocks(const Grid& g);
 // vb_stage_f32.cu): WENOZ reconstruction with HLL or HLLC
 inline bool zp_available(int rec, int rs) { return rec == 2 && (rs == 0 || rs == 1); }
 cudaError_t launch_stage_zp(int rs, const StageParams& p, const StageBufs<float>& b, cudaStream_t s);
-// tensor map of one FP32 SoA state array for the TMA form of the z-pair kernel
-// (out: a 64-byte aligned CUtensorMap); false if the layout does not allow one
-bool encode_plane_tmap(void* out, const float* P, const Grid& g);
+// tensor map of one SoA state array for the TMA forms of the stage kernels
+// (3D FP32: the z-pair kernel's plane boxes; 2D: k_stage's tile boxes; out: a
+// 64-byte aligned CUtensorMap); false where no TMA form exists or the layout
+// does not allow one
+template <typename R> bool encode_stage_tmap(void* out, const R* P, const Grid& g);
 // 1 when launch_stage with these arguments leaves the FP32 divergence in Pout
 // for the caller's con2prim kernel (z-pair kernel with skip_c2p and want_div)
 template <typename R> int stage_div_in_pout(int dims, int rec, int rs, const StageParams& p);

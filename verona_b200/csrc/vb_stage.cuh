@@ -11,11 +11,16 @@
 // fluxes in shared memory and accumulates the flux difference into per-cell
 // FP64 registers. Face states and fluxes never reach HBM. It then applies the
 // RK combination, solves con2prim with the cell's previous primitive state as
-// the guess and writes U and the floored P.
+// the guess and writes U and the floored P. In 2D the tile with its halo
+// along both axes can instead come as one TMA tile (TMA form of k_stage).
 #pragma once
+#include <cuda.h>  // CUtensorMap
+
 #include "vb_con2prim.cuh"
 #include "vb_index.cuh"
 #include "vb_internal.h"
+#include "vb_tc.cuh"
+#include "vb_tmap.h"
 
 namespace vb {
 
@@ -40,6 +45,34 @@ template <int DIM, int TX, int TY, int TZ> struct TileGeom {
         return sizeof(R) * NV * (size_t)(EXTMAX + 2 * FACEMAX);
     }
 };
+
+// TMA form of the 2D tile: one box of the tile with its 3-cell halo on both
+// axes, every variable, [NV][TY + 6][BXW] (x fastest). The box starts at
+// x = x0 - 3 = TX * blockIdx.x, 16-byte aligned for TX a multiple of 4, and
+// is TX + 6 cells rounded up to a 16-byte row wide.
+template <typename R, int TX, int TY> struct TmaTile2 {
+    static constexpr int NV = 4;
+    static constexpr int BXW = (TX + 6 + 16 / (int)sizeof(R) - 1) / (16 / (int)sizeof(R)) * (16 / (int)sizeof(R));
+    static constexpr int BY = TY + 6;
+    static constexpr int BOXE = BXW * BY;  // elements per variable
+    static constexpr int BOX_BYTES = (int)sizeof(R) * NV * BOXE;
+    static constexpr int FACEMAX = (TX + 1) * TY > TX * (TY + 1) ? (TX + 1) * TY : TX * (TY + 1);
+    static constexpr size_t smem_bytes() {
+        return 128 + (size_t)(BOX_BYTES + 127) / 128 * 128 + sizeof(R) * NV * (size_t)(2 * FACEMAX) + 16;
+    }
+};
+constexpr uint32_t TILE_MAX_POLLS = 1u << 22;  // bounded wait for the TMA tile
+
+// tensor map of a 2D state array for the TMA form of k_stage: dims (x, y,
+// variable) with byte strides (sy, vs) x element size; the box is TmaTile2's
+template <typename R, int TX, int TY> bool encode_tile2_tmap(void* out, const R* P, const Grid& g) {
+    using TT = TmaTile2<R, TX, TY>;
+    if (g.dims != 2 || g.nv != TT::NV) return false;
+    const cuuint64_t dim[3] = {(cuuint64_t)g.n[0], (cuuint64_t)g.n[1], (cuuint64_t)TT::NV};
+    const cuuint64_t stride[2] = {(cuuint64_t)g.sy * sizeof(R), (cuuint64_t)g.vs * sizeof(R)};
+    const cuuint32_t box[3] = {(cuuint32_t)TT::BXW, (cuuint32_t)TT::BY, (cuuint32_t)TT::NV};
+    return encode_tmap(out, P, (int)sizeof(R), 3, dim, stride, box);
+}
 
 __device__ __forceinline__ void count_add(unsigned long long* c, int which, unsigned long long v) {
     if (c && v) atomicAdd(c + which, v);
@@ -138,17 +171,27 @@ template <bool CG, typename T> __device__ __forceinline__ T ld_in(const T* p) {
 }
 
 // One TX x TY x TZ tile of a stage (tile coordinates bx, by, bz); the body of
-// k_stage, shared with the batched kernel. smem_raw: TileGeom::smem_bytes<R>().
-template <int DIM, int REC, int RS, typename R, int TX, int TY, int TZ, int NT, bool CG>
+// k_stage, shared with the batched kernel. smem_raw: TileGeom::smem_bytes<R>(),
+// or TmaTile2::smem_bytes() for the TMA form (2D; tm: the tensor map of Pin,
+// dims (x, y, variable)), which loads the tile once for both axes.
+template <int DIM, int REC, int RS, typename R, int TX, int TY, int TZ, int NT, bool CG, bool TMA = false>
 __device__ __forceinline__ void stage_tile(const StageParams& p, const StageBufs<R>& b, int bx, int by, int bz,
-                                           unsigned char* smem_raw) {
+                                           unsigned char* smem_raw, const CUtensorMap* tm = nullptr) {
     using G = TileGeom<DIM, TX, TY, TZ>;
+    using TT = TmaTile2<R, TX, TY>;
+    static_assert(!TMA || (DIM == 2 && TZ == 1 && (TX * (int)sizeof(R)) % 16 == 0), "TMA tiles: 2D");
     constexpr int NV = G::NV;
     constexpr int TC = G::TC;
     constexpr int CPT = (TC + NT - 1) / NT;
-    R* sP = reinterpret_cast<R*>(smem_raw);
-    R* sL = sP + NV * G::EXTMAX;
-    R* sR = sL + NV * G::FACEMAX;
+    R* sP;
+    uint64_t* sBar = nullptr;
+    if constexpr (TMA)
+        sP = reinterpret_cast<R*>(smem_raw + ((128u - (tc::smem_u32(smem_raw) & 127u)) & 127u));
+    else
+        sP = reinterpret_cast<R*>(smem_raw);
+    R* sL = TMA ? sP + (TT::BOX_BYTES + 127) / 128 * 128 / (int)sizeof(R) : sP + NV * G::EXTMAX;
+    R* sR = sL + NV * (TMA ? TT::FACEMAX : G::FACEMAX);
+    if constexpr (TMA) sBar = reinterpret_cast<uint64_t*>(((uintptr_t)(sR + NV * TT::FACEMAX) + 7) & ~(uintptr_t)7);
 
     const int tid = threadIdx.x;
     const int T[3] = {TX, TY, TZ};
@@ -172,23 +215,47 @@ __device__ __forceinline__ void stage_tile(const StageParams& p, const StageBufs
         for (int v = 0; v < NV; ++v) acc[c][v] = ok ? ld_in<CG>(b.Us + v * vs + gidx) : 0.0;
     }
 
+    if constexpr (TMA) {
+        // the tile with its halo on both axes, every variable, as one TMA box
+        if (tid == 0) {
+            tc::mbar_init(sBar, 1);
+            tc::fence_mbar_init();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            tc::mbar_arrive_expect_tx(sBar, TT::BOX_BYTES);
+            tc::tma_load_3d(sP, tm, org[0] - NG, org[1] - NG, 0, sBar);
+        }
+        const bool ok = tc::mbar_wait(sBar, 0, nullptr, TILE_MAX_POLLS);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) count_add(p.counters, CNT_TIMEOUT, 1);
+            return;
+        }
+    }
+
 #pragma unroll 1
     for (int d = 0; d < DIM; ++d) {
-        const int EX = TX + (d == 0 ? 6 : 0), EY = TY + (d == 1 ? 6 : 0), EZ = TZ + (d == 2 ? 6 : 0);
+        // staged tile: EX x EY x EZ elements per variable; the TMA tile is the
+        // same BXW x (TY + 6) box for both axes, the cell (0, 0) at (3, 3)
+        const int EX = TMA ? TT::BXW : TX + (d == 0 ? 6 : 0), EY = TMA ? TT::BY : TY + (d == 1 ? 6 : 0),
+                  EZ = TMA ? 1 : TZ + (d == 2 ? 6 : 0);
         const int EXT = EX * EY * EZ;
         const int ox = org[0] - (d == 0 ? NG : 0), oy = org[1] - (d == 1 ? NG : 0),
                   oz = org[2] - (d == 2 ? NG : 0);
         __syncthreads();
         // 1. stage the axis-extended tile of P
-        for (int e = tid; e < NV * EXT; e += NT) {
-            int v = e / EXT, r = e - v * EXT;
-            int ex = r % EX, ey = (r / EX) % EY, ez = r / (EX * EY);
-            int gi = ox + ex, gj = oy + ey, gk = oz + ez;
-            R val = R(0);
-            if (gi < p.n[0] && gj < p.n[1] && gk < p.n[2]) val = ld_in<CG>(b.Pin + v * vs + gi + p.sy * gj + p.sz * gk);
-            sP[v * EXT + r] = val;
+        if constexpr (!TMA) {
+            for (int e = tid; e < NV * EXT; e += NT) {
+                int v = e / EXT, r = e - v * EXT;
+                int ex = r % EX, ey = (r / EX) % EY, ez = r / (EX * EY);
+                int gi = ox + ex, gj = oy + ey, gk = oz + ez;
+                R val = R(0);
+                if (gi < p.n[0] && gj < p.n[1] && gk < p.n[2])
+                    val = ld_in<CG>(b.Pin + v * vs + gi + p.sy * gj + p.sz * gk);
+                sP[v * EXT + r] = val;
+            }
+            __syncthreads();
         }
-        __syncthreads();
         // 2. reconstruct each cell of the tile (plus one halo cell on each side
         //    along d) once; store its two face values, floored
         const int FX = TX + (d == 0), FY = TY + (d == 1), FZ = TZ + (d == 2);
@@ -204,7 +271,8 @@ __device__ __forceinline__ void stage_tile(const StageParams& p, const StageBufs
             for (int a = 0; a < 3; ++a)
                 ok = ok && (a == d ? (c[a] >= -1 && c[a] <= vt[a]) : c[a] < vt[a]);
             if (!ok) continue;
-            int ex = c[0] + (d == 0 ? NG : 0), ey = c[1] + (d == 1 ? NG : 0), ez = c[2] + (d == 2 ? NG : 0);
+            int ex = c[0] + (d == 0 || TMA ? NG : 0), ey = c[1] + (d == 1 || TMA ? NG : 0),
+                ez = c[2] + (d == 2 ? NG : 0);
             int base = ex + EX * (ey + EY * ez);
             int fR = c[0] + FX * (c[1] + FY * c[2]);                    // face c_d
             int fL = fR + (d == 0 ? 1 : (d == 1 ? FX : FX * FY));         // face c_d + 1
@@ -304,19 +372,24 @@ __device__ __forceinline__ void stage_tile(const StageParams& p, const StageBufs
     }
 }
 
-template <int DIM, int REC, int RS, typename R, int TX, int TY, int TZ, int NT>
-__global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b) {
+template <int DIM, int REC, int RS, typename R, int TX, int TY, int TZ, int NT, bool TMA>
+__global__ void __launch_bounds__(NT) k_stage(StageParams p, StageBufs<R> b, const __grid_constant__ CUtensorMap tm) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    stage_tile<DIM, REC, RS, R, TX, TY, TZ, NT, false>(p, b, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z,
-                                                       smem_raw);
+    stage_tile<DIM, REC, RS, R, TX, TY, TZ, NT, false, TMA>(p, b, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z,
+                                                            smem_raw, &tm);
 }
 
-template <int DIM, int REC, int RS, typename R>
-cudaError_t launch_stage_t(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
+// TMA form where the caller encoded a tensor map of Pin (p.tmap_in; 2D)
+template <int DIM, int REC, int RS, typename R, bool TMA>
+cudaError_t launch_stage_tt(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
     using C = TileCfg<DIM>;
     using G = TileGeom<DIM, C::TX, C::TY, C::TZ>;
-    auto kern = k_stage<DIM, REC, RS, R, C::TX, C::TY, C::TZ, C::NT>;
-    const size_t smem = G::template smem_bytes<R>();
+    auto kern = k_stage<DIM, REC, RS, R, C::TX, C::TY, C::TZ, C::NT, TMA>;
+    size_t smem;
+    if constexpr (TMA)
+        smem = TmaTile2<R, C::TX, C::TY>::smem_bytes();
+    else
+        smem = G::template smem_bytes<R>();
     static unsigned long long attr_set = 0;  // one bit per device, per instantiation
     int dev = 0;
     cudaGetDevice(&dev);
@@ -329,8 +402,20 @@ cudaError_t launch_stage_t(const StageParams& p, const StageBufs<R>& b, cudaStre
     }
     dim3 grid((p.n[0] - 2 * NG + C::TX - 1) / C::TX, DIM > 1 ? (p.n[1] - 2 * NG + C::TY - 1) / C::TY : 1,
               DIM > 2 ? (p.n[2] - 2 * NG + C::TZ - 1) / C::TZ : 1);
-    kern<<<grid, C::NT, smem, s>>>(p, b);
+    CUtensorMap tm;
+    if (TMA)
+        tm = *static_cast<const CUtensorMap*>(p.tmap_in);
+    else
+        memset(&tm, 0, sizeof tm);
+    kern<<<grid, C::NT, smem, s>>>(p, b, tm);
     return cudaGetLastError();
+}
+template <int DIM, int REC, int RS, typename R>
+cudaError_t launch_stage_t(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
+    if constexpr (DIM == 2) {
+        if (p.tmap_in) return launch_stage_tt<DIM, REC, RS, R, true>(p, b, s);
+    }
+    return launch_stage_tt<DIM, REC, RS, R, false>(p, b, s);
 }
 
 template <int DIM, typename R>

@@ -5,6 +5,10 @@
 
 namespace vb {
 VB_INSTANTIATE_LAUNCHERS(double)
+// tensor map of an FP64 state array: the box tile of k_stage in 2D
+template <> bool encode_stage_tmap<double>(void* out, const double* P, const Grid& g) {
+    return g.dims == 2 && encode_tile2_tmap<double, TileCfg<2>::TX, TileCfg<2>::TY>(out, P, g);
+}
 template cudaError_t launch_c2p<double>(const StageParams&, const StageBufs<double>&, cudaStream_t);
 
 // ---- point kernels: the device physics on arrays of independent states

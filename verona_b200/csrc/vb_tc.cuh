@@ -118,6 +118,15 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, int c0,
         : "memory");
 }
 
+// the same for a 3D tensor map
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int c0, int c1, int c2, uint64_t* mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(mbar))
+        : "memory");
+}
+
 // bounded wait for phase `parity` of an mbarrier; false (and *err set) on timeout
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, unsigned int* err, uint32_t max_polls) {
     const uint32_t a = smem_u32(mbar);
