@@ -407,6 +407,7 @@ def run_ours(args, rank, world, dist):
         mlp.attach(s)
     s.set_tuning(learned_fused=int(args.learned_form == "fused"), fp32_pairs=int(args.stencil == "pairs"),
                  tma_tiles=int(args.planes == "tma"))
+    tma_active = s.tma_tiles_active
     s.load_prims(P0)
     with Clocks(torch.cuda.current_device()) as clk:
         ms, st_ms, st_l, launches = timed_steps(s, dt, W, K, dist)
@@ -499,7 +500,8 @@ def run_ours(args, rank, world, dist):
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 bulk + f64 (U, con2prim)", "data": "synthetic",
         "config": dict(workload_config(n, guess), learned_form=args.learned_form if learned_ok else None,
-                       stencil=args.stencil, planes=args.planes if args.stencil == "pairs" else None),
+                       stencil=args.stencil, planes=args.planes if args.stencil == "pairs" else None,
+                       tma_tiles_active=tma_active),
         "fp64_plain": fp64,
         "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
         "l1_error_vs_fp64": err,
@@ -665,6 +667,7 @@ def run_jet2d(args, rank, world, dist):
             s = Solver(2, (n, n), GAMMA, (dx, dx), recon="wenoz", riemann="hllc", rk=3, precision=prec, n_iter=50,
                        tol=1e-12, floor=1e-8)
             s.set_tuning(tma_tiles=tma)
+            tma_active = s.tma_tiles_active
             s.set_boundary(0, 2, [32.0, n / 2, 0.0, 0.01, 1e-3 / (GAMMA - 1), math.sqrt(99.0), 0.0, 0.0])
             s.init_prims("ambient", seed=7 + rank, noise=0.03, rho=1.0, u=1e-3 / (GAMMA - 1))
             ms, st_ms, st_l, launches = timed_steps(s, dt, W, K, dist)
@@ -674,6 +677,7 @@ def run_jet2d(args, rank, world, dist):
             c = s.counters()
             res[prec] = {"value": world * n * n * K / (t.item() / 1e3), "ms_per_step": t.item() / K,
                          "stage_ms_per_launch": st_ms / max(st_l, 1), "c2p_failures": int(c[0]),
+                         "tma_tiles_active": tma_active,
                          "tma_timeouts": int(c[4])}
             del s
     if rank != 0:

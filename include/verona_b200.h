@@ -226,6 +226,10 @@ typedef struct vb_tuning {
 } vb_tuning;
 int vb_set_tuning(vb_handle h, const vb_tuning* t);
 int vb_get_tuning(vb_handle h, vb_tuning* t);
+/* *active = 1 if vb_step stages the stencil tiles by TMA on this handle: the
+ * tuning allows it (tma_tiles != 0) and both state buffers have a tensor map
+ * (3D FP32 bulk, 2D); the z-pair kernel must also be the 3D kernel in use. */
+int vb_tma_tiles_active(vb_handle h, int* active);
 
 /* Device bytes held by the handle. */
 int vb_memory_bytes(vb_handle h, uint64_t* bytes);

@@ -211,6 +211,7 @@ def test_learned_path_tma_tiles_match_cp_async_planes(net):
                    n_iter=50, tol=1e-12, floor=1e-8)
         net.attach(s)
         s.set_tuning(learned_fused=1, fp32_pairs=1, tma_tiles=tma)
+        assert s.tma_tiles_active == bool(tma)
         s.set_boundary(0, 2, nozzle_params(3, n, 4.0, gamma=G))
         s.load_prims(P0)
         s.step(dt, 4)

@@ -347,6 +347,7 @@ def test_tma_tiles_match_cp_async_planes_bitwise(rs, variant):
         s = Solver(3, n, g, dxs, recon="wenoz", riemann=rs, rk=3, precision="fp32", n_iter=50, tol=1e-12, floor=1e-8)
         s.set_tuning(split_con2prim=int(variant == "split"), fp32_pairs=1, tma_tiles=tma)
         assert s.get_tuning()["tma_tiles"] == tma
+        assert s.tma_tiles_active == bool(tma)
         s.set_boundary(0, 2, nozzle_params(3, n, 5.0, gamma=g))
         s.load_prims(P0)
         s.step(dt, 5)
@@ -379,6 +380,7 @@ def test_2d_tma_tiles_match_loaded_tiles_bitwise(precision, rec, rs):
         s = Solver(2, n[:2], g, dxs, recon=rec, riemann=rs, rk=3, precision=precision, n_iter=50, tol=1e-12,
                    floor=1e-8)
         s.set_tuning(tma_tiles=tma)
+        assert s.tma_tiles_active == bool(tma)
         s.set_boundary(0, 2, nozzle_params(2, n, 3.0, gamma=g))
         s.load_prims(P0)
         s.step(dt, 6)

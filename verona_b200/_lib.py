@@ -92,6 +92,7 @@ _SIGS = {
     "vb_get_counters": [_vp, C.POINTER(C.c_uint64), C.c_int, _vp],
     "vb_reset_counters": [_vp, _vp],
     "vb_memory_bytes": [_vp, C.POINTER(C.c_uint64)],
+    "vb_tma_tiles_active": [_vp, C.POINTER(C.c_int)],
     "vb_profile_enable": [_vp, C.c_int],
     "vb_profile_read": [_vp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
     "vb_profile_read2": [_vp, _dp, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],

@@ -760,6 +760,12 @@ int vb_get_tuning(vb_handle h, vb_tuning* t) {
     return VB_OK;
 }
 
+int vb_tma_tiles_active(vb_handle h, int* active) {
+    if (!h || !active) return fail(h, VB_ERR_ARG, "vb_tma_tiles_active: null argument");
+    *active = h->tun.tma_tiles != 0 && h->tmap_ok[0] && h->tmap_ok[1] ? 1 : 0;
+    return VB_OK;
+}
+
 int vb_memory_bytes(vb_handle h, uint64_t* bytes) {
     if (!h || !bytes) return fail(h, VB_ERR_ARG, "vb_memory_bytes: null argument");
     *bytes = h->bytes;

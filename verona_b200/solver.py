@@ -202,6 +202,13 @@ class Solver:
         return ms.value, st.value, sl.value, al.value
 
     @property
+    def tma_tiles_active(self) -> bool:
+        """True if the stencil tiles are staged by TMA on this handle."""
+        v = C.c_int()
+        L.check(L.lib().vb_tma_tiles_active(self._h, C.byref(v)), self._h)
+        return bool(v.value)
+
+    @property
     def memory_bytes(self) -> int:
         v = C.c_uint64()
         L.check(L.lib().vb_memory_bytes(self._h, C.byref(v)), self._h)
