@@ -51,7 +51,7 @@ def parse():
                     help="fp64: time only the plain FP64 path (profiling runs)")
     ap.add_argument("--guess", default="auto", choices=["auto", "learned", "previous"],
                     help="con2prim guess of the fast path (auto: learned when the network is available)")
-    ap.add_argument("--learned-form", default="fused", choices=["fused", "two", "pipelined"],
+    ap.add_argument("--learned-form", default="fused", choices=["fused", "two"],
                     help="learned con2prim as one kernel (guess + Newton) or as a guess kernel + con2prim kernel")
     ap.add_argument("--stencil", default="pairs", choices=["pairs", "scalar"],
                     help="FP32 stencil kernel: two cells per thread on packed FP32 pairs, or one cell per thread")
@@ -405,8 +405,7 @@ def run_ours(args, rank, world, dist):
     s = make_solver(n, "fp32", guess)
     if learned_ok:
         mlp.attach(s)
-    s.set_tuning(learned_fused={"two": 0, "fused": 1, "pipelined": 2}[args.learned_form],
-                 fp32_pairs=int(args.stencil == "pairs"),
+    s.set_tuning(learned_fused=int(args.learned_form == "fused"), fp32_pairs=int(args.stencil == "pairs"),
                  tma_tiles=int(args.planes == "tma"))
     tma_active = s.tma_tiles_active
     s.load_prims(P0)
@@ -493,7 +492,7 @@ def run_ours(args, rank, world, dist):
     bytes_per_cell_step = 440.0
     stage_ms_per_launch = st_ms / max(st_l, 1)
     achieved = cells * bytes_per_cell_step / 3.0 / (stage_ms_per_launch / 1e3) / 1e9
-    form = "_fused" if learned_ok and args.learned_form in ("fused", "pipelined") else ""
+    form = "_fused" if learned_ok and args.learned_form == "fused" else ""
     form += "_pairs" if args.stencil == "pairs" else ""
     traffic = read_traffic(f"fp32_{guess}{form}_stage_group")
     line = {
@@ -511,10 +510,10 @@ def run_ours(args, rank, world, dist):
                      "per": "one RK-stage launch of the kernel group over the full grid",
                      "kernel": ("k_stage_zp (z-pair FP32 reconstruct+HLLC+divergence) + k_c2p_learned "
                                 "(RK combination, tensor-core guess, W Newton)" if learned_ok and
-                                args.learned_form in ("fused", "pipelined") else "stencil kernel + con2prim kernel(s)"),
+                                args.learned_form == "fused" else "stencil kernel + con2prim kernel(s)"),
                      "algorithmic_bytes_per_launch": bytes_per_cell_step / 3.0 * cells,
                      "stage_ms_per_launch": stage_ms_per_launch},
-        "roofline_fp32": fp32_roofline(cells, stencil_ms, learned_ok and args.learned_form in ("fused", "pipelined")
+        "roofline_fp32": fp32_roofline(cells, stencil_ms, learned_ok and args.learned_form == "fused"
                                        and args.stencil == "pairs"),
         "gpu_launches": launches,
         "clocks": clk.summary,

@@ -203,10 +203,8 @@ int vb_reset_counters(vb_handle h, void* stream);
  * default. force_box: 1 = use the box-tile stencil kernel for 3D even where
  * the z-marching kernel fits. Results are identical for every variant.
  * learned_fused (guess = VB_GUESS_LEARNED only): 1 = the network's guess and
- * the W Newton from it run in one kernel; 2 = the same kernel software-
- * pipelined (each 128-cell tile's Newton runs while the next tile's first
- * MMA is in flight), identical results; 0 = a guess kernel writes one W per
- * cell and the con2prim kernel reads it; -1 = library default (1). All start
+ * the W Newton from it run in one kernel; 0 = a guess kernel writes one W per
+ * cell and the con2prim kernel reads it; -1 = library default (1). Both start
  * the Newton from the same FP32-rounded guess.
  * fp32_pairs (precision = VB_PREC_FP32_BULK, 3D, WENOZ with HLL or HLLC): 1 =
  * the z-pair stencil kernel (two cells per thread on packed FP32 pairs);

@@ -193,39 +193,6 @@ def test_learned_fused_kernel_matches_two_kernel_form(net, precision):
     assert max(l1) < (1e-12 if precision == "fp64" else 2e-6)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_pipelined_learned_kernel_matches_fused_kernel(net, precision):
-    """The software-pipelined fused learned con2prim (each tile's W Newton runs
-    while the next tile's first MMA is in flight) against the fused kernel:
-    every cell gets the same guess and the same Newton, so P, U and the
-    iteration statistics agree exactly. 21 cells in z and 21 x 64 x 24 cells in
-    all leave a partial last tile."""
-    from helpers import jet_ic, nozzle_params
-    from verona_b200 import Solver
-
-    n = (64, 24, 21)
-    P0 = jet_ic(3, n, gamma=G, noise=0.03, seed=13)
-    dxs = [1.0 / 64] * 3
-    dt = 0.4 / sum(1.0 / d for d in dxs)
-    out = {}
-    for form in (1, 2):
-        s = Solver(3, n, G, dxs, recon="wenoz", riemann="hllc", rk=3, guess="learned", precision=precision,
-                   n_iter=50, tol=1e-12, floor=1e-8, stats=1)
-        net.attach(s)
-        s.set_tuning(learned_fused=form)
-        assert s.get_tuning()["learned_fused"] == form
-        s.set_boundary(0, 2, nozzle_params(3, n, 4.0, gamma=G))
-        s.load_prims(P0)
-        s.step(dt, 4)
-        out[form] = (s.prims(), s.cons(), s.counters())
-    c1, c2 = out[1][2], out[2][2]
-    print(precision, "fused counters", c1.tolist(), "pipelined", c2.tolist())
-    assert c2[0] == 0 and c2[4] == 0
-    assert np.array_equal(c1, c2)
-    assert np.array_equal(out[1][0], out[2][0])
-    assert np.array_equal(out[1][1], out[2][1])
-
-
 def test_learned_path_tma_tiles_match_cp_async_planes(net):
     """The headline form (z-pair stencil leaving the FP32 divergence, fused
     learned con2prim) with the stencil's planes brought in as TMA tiles and

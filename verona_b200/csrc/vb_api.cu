@@ -591,7 +591,7 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
             q.c2p_mode = C2P_GUESS_W;
             q.div_in_pout = stage_div_in_pout<R>(h->dims, h->opt.recon, h->opt.riemann, p);
             if (h->tun.learned_fused != 0) {
-                VB_CUDA(h, launch_c2p_learned<R>(h->mlp_blob, q, bufs, h->tc_err, s, h->tun.learned_fused == 2));
+                VB_CUDA(h, launch_c2p_learned<R>(h->mlp_blob, q, bufs, h->tc_err, s));
                 h->launches += 1;
             } else {
                 VB_CUDA(h, launch_mlp_guess(h->mlp_blob, p, Uo, h->w_guess, h->tc_err, s));
@@ -745,11 +745,11 @@ int vb_attach_mlp(vb_handle h, vb_mlp_handle m) {
 int vb_set_tuning(vb_handle h, const vb_tuning* t) {
     if (!h || !t) return fail(h, VB_ERR_ARG, "vb_set_tuning: null argument");
     if (t->split_con2prim < -1 || t->split_con2prim > 1 || t->force_box < 0 || t->force_box > 1 ||
-        t->learned_fused < -1 || t->learned_fused > 2 || t->fp32_pairs < -1 || t->fp32_pairs > 1 ||
+        t->learned_fused < -1 || t->learned_fused > 1 || t->fp32_pairs < -1 || t->fp32_pairs > 1 ||
         t->tma_tiles < -1 || t->tma_tiles > 1)
         return fail(h, VB_ERR_ARG,
-                    "vb_set_tuning: split_con2prim in {-1,0,1}, force_box in {0,1}, learned_fused in {-1,0,1,2}, "
-                    "fp32_pairs and tma_tiles in {-1,0,1}");
+                    "vb_set_tuning: split_con2prim in {-1,0,1}, force_box in {0,1}, learned_fused, fp32_pairs and "
+                    "tma_tiles in {-1,0,1}");
     h->tun = *t;
     return VB_OK;
 }

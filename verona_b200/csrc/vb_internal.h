@@ -135,10 +135,9 @@ cudaError_t launch_mlp_guess(const void* mlp_blob, const StageParams& p, const d
                              unsigned int* err, cudaStream_t s);
 // the same guess and the W Newton from it in one kernel (vb_mlp.cu): U of the
 // stage in, the floored P of every interior cell out
-// (pipelined: each tile's Newton overlaps the next tile's first MMA)
 template <typename R>
 cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const StageBufs<R>& b, unsigned int* err,
-                               cudaStream_t s, bool pipelined);
+                               cudaStream_t s);
 
 // point kernels (FP64, vb_stage_f64.cu)
 cudaError_t launch_point_recon(int method, const double* q, double* out, int n, cudaStream_t s);

@@ -290,11 +290,8 @@ __device__ __forceinline__ void store_row64_relu(__nv_bfloat16* buf, int row, co
 // One MLP forward for the CTA's 128 cells (thread t = cell / row t). f: this
 // thread's 4 normalised features; returns y, the predicted p / E. The caller
 // holds TMEM (64 columns at s.tmem_base) and the mbarrier; `phase` counts
-// completed commits. work() runs in every thread while the first layer's MMA
-// is in flight. Returns false if a bounded wait ran out.
-template <typename Work>
-__device__ __forceinline__ bool mlp_forward_tile_w(InferSmem& s, const float* f, float& y, uint32_t& phase,
-                                                   unsigned int* err, Work&& work) {
+// completed commits. Returns false if a bounded wait ran out.
+__device__ bool mlp_forward_tile(InferSmem& s, const float* f, float& y, uint32_t& phase, unsigned int* err) {
     const int t = threadIdx.x, warp = t >> 5;
     const uint32_t tmem = s.tmem_base;
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
@@ -314,7 +311,6 @@ __device__ __forceinline__ bool mlp_forward_tile_w(InferSmem& s, const float* f,
         tc::mma_bf16(tmem, tc::operand_desc(s.h, TILE, 0), tc::operand_desc(s.w1i, MLP_H, 0), ID64, 0);
         tc::mma_commit(&s.mbar);
     }
-    work();
     if (!cta_wait(&s.mbar, phase & 1, err)) return false;
     ++phase;
     tc::fence_after_sync();
@@ -362,9 +358,6 @@ __device__ __forceinline__ bool mlp_forward_tile_w(InferSmem& s, const float* f,
     tc::fence_before_sync();
     __syncthreads();  // all TMEM loads of this tile done before the next tile's MMA
     return true;
-}
-__device__ bool mlp_forward_tile(InferSmem& s, const float* f, float& y, uint32_t& phase, unsigned int* err) {
-    return mlp_forward_tile_w(s, f, y, phase, err, [] {});
 }
 
 // shared prologue / epilogue of the inference kernels: weights, TMEM, mbarrier.
@@ -834,10 +827,7 @@ cudaError_t launch_mlp_guess(const void* mlp_blob, const StageParams& p, const d
 // divergence in Pout, and this kernel forms U = rk_a U0 + rk_b (Us - div)
 // (written to Uo) before the features; the next tile's inputs are loaded
 // before the current tile's Newton, whose latency covers them.
-// PIPE: software-pipelined form; each tile's Newton runs one iteration later,
-// while the next tile's first MMA is in flight, after the loads of the tile
-// after that are issued. Every cell's arithmetic is the same in both forms.
-template <typename R, bool PIPE>
+template <typename R>
 __global__ void __launch_bounds__(TILE, 5) k_c2p_learned(const MlpBlob* __restrict__ blob, StageParams p,
                                                          StageBufs<R> b, unsigned int* err) {
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -883,21 +873,6 @@ __global__ void __launch_bounds__(TILE, 5) k_c2p_learned(const MlpBlob* __restri
         }
     };
     unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
-    // the W Newton from the network's guess y, floors, P of cell cc
-    auto newton = [&](const double* uu, float yy, long long cc) {
-        const double W0 = (double)(float)(-uu[1] * (1.0 + (double)fmaxf(yy, 0.0f)));
-        double P[5];
-        int fb;
-        const int r = c2p_w(p.gamma, uu, W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, P, &fb);
-        n_fail += (r < 0);
-        n_fb += fb;
-        n_it += (r < 0 ? -r : r);
-        n_cells += 1;
-        P[0] = jmax(P[0], p.floor_);
-        P[1] = jmax(P[1], p.floor_);
-#pragma unroll
-        for (int v = 0; v < 5; ++v) b.Pout[v * vs + cc] = (R)P[v];
-    };
     uint32_t phase = 0;
     long long tile = blockIdx.x;
     long long c = 0;
@@ -908,51 +883,33 @@ __global__ void __launch_bounds__(TILE, 5) k_c2p_learned(const MlpBlob* __restri
         load(c, r);
         form(r, c, u);
     }
-    if constexpr (!PIPE) {
-        for (; tile < ntiles; tile += gridDim.x) {
-            const long long nt = tile + gridDim.x;
-            long long cn = 0;
-            const bool okn = nt < ntiles && cell(nt * TILE + t, cn);
-            float f[4];
-            guess_features(u, (float)p.gamma, s.mu, s.isd, f);
-            float y = 0.f;
-            if (!mlp_forward_tile(s, f, y, phase, err)) break;
-            Raw rn;
-            if (okn) load(cn, rn);
-            if (ok) newton(u, y, c);
-            if (okn) form(rn, cn, u);
-            ok = okn;
-            c = cn;
-        }
-    } else {
-        double up[5] = {1.0, -2.0, 0.0, 0.0, 0.0};  // the previous tile's cell, its guess and index
-        float yp = 0.f;
-        long long cp = 0;
-        bool okp = false;
-        for (; tile < ntiles; tile += gridDim.x) {
-            const long long nt = tile + gridDim.x;
-            long long cn = 0;
-            const bool okn = nt < ntiles && cell(nt * TILE + t, cn);
-            float f[4];
-            guess_features(u, (float)p.gamma, s.mu, s.isd, f);
-            float y = 0.f;
-            Raw rn;
-            auto work = [&] {
-                if (okn) load(cn, rn);
-                if (okp) newton(up, yp, cp);
-                okp = false;
-            };
-            if (!mlp_forward_tile_w(s, f, y, phase, err, work)) break;
-            okp = ok;
-            cp = c;
-            yp = y;
+    for (; tile < ntiles; tile += gridDim.x) {
+        const long long nt = tile + gridDim.x;
+        long long cn = 0;
+        const bool okn = nt < ntiles && cell(nt * TILE + t, cn);
+        float f[4];
+        guess_features(u, (float)p.gamma, s.mu, s.isd, f);
+        float y = 0.f;
+        if (!mlp_forward_tile(s, f, y, phase, err)) break;
+        Raw rn;
+        if (okn) load(cn, rn);
+        if (ok) {
+            const double W0 = (double)(float)(-u[1] * (1.0 + (double)fmaxf(y, 0.0f)));
+            double P[5];
+            int fb;
+            const int r = c2p_w(p.gamma, u, W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, P, &fb);
+            n_fail += (r < 0);
+            n_fb += fb;
+            n_it += (r < 0 ? -r : r);
+            n_cells += 1;
+            P[0] = jmax(P[0], p.floor_);
+            P[1] = jmax(P[1], p.floor_);
 #pragma unroll
-            for (int v = 0; v < 5; ++v) up[v] = u[v];
-            if (okn) form(rn, cn, u);
-            ok = okn;
-            c = cn;
+            for (int v = 0; v < 5; ++v) b.Pout[v * vs + c] = (R)P[v];
         }
-        if (okp) newton(up, yp, cp);
+        if (okn) form(rn, cn, u);
+        ok = okn;
+        c = cn;
     }
     infer_end(s);
     unsigned long long* cnt = p.counters;
@@ -974,19 +931,19 @@ __global__ void __launch_bounds__(TILE, 5) k_c2p_learned(const MlpBlob* __restri
     }
 }
 
-template <typename R, bool PIPE>
-cudaError_t launch_c2p_learned_t(const void* mlp_blob, const StageParams& p, const StageBufs<R>& b, unsigned int* err,
-                                 cudaStream_t s) {
+template <typename R>
+cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const StageBufs<R>& b, unsigned int* err,
+                               cudaStream_t s) {
     static unsigned long long attr = 0;
     static int resident[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     const int d = dev & 63;
     if (!(attr >> d & 1ULL)) {
-        cudaError_t e = cudaFuncSetAttribute(k_c2p_learned<R, PIPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_c2p_learned<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)sizeof(InferSmem));
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(k_c2p_learned<R, PIPE>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        e = cudaFuncSetAttribute(k_c2p_learned<R>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         // 5 CTAs per SM: the launch bound (96 registers x 128 threads), 5 x 43 KB of
         // shared memory and 5 x 64 TMEM columns all fit (the occupancy query
@@ -1003,19 +960,13 @@ cudaError_t launch_c2p_learned_t(const void* mlp_blob, const StageParams& p, con
     const long long tiles = (cells + TILE - 1) / TILE;
     const int nb = (int)std::min<long long>(tiles, resident[d]);
     if (nb <= 0) return cudaSuccess;
-    k_c2p_learned<R, PIPE><<<nb, TILE, sizeof(InferSmem), s>>>((const MlpBlob*)mlp_blob, p, b, err);
+    k_c2p_learned<R><<<nb, TILE, sizeof(InferSmem), s>>>((const MlpBlob*)mlp_blob, p, b, err);
     return cudaGetLastError();
 }
-template <typename R>
-cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const StageBufs<R>& b, unsigned int* err,
-                               cudaStream_t s, bool pipelined) {
-    return pipelined ? launch_c2p_learned_t<R, true>(mlp_blob, p, b, err, s)
-                     : launch_c2p_learned_t<R, false>(mlp_blob, p, b, err, s);
-}
 template cudaError_t launch_c2p_learned<float>(const void*, const StageParams&, const StageBufs<float>&,
-                                               unsigned int*, cudaStream_t, bool);
+                                               unsigned int*, cudaStream_t);
 template cudaError_t launch_c2p_learned<double>(const void*, const StageParams&, const StageBufs<double>&,
-                                                unsigned int*, cudaStream_t, bool);
+                                                unsigned int*, cudaStream_t);
 }  // namespace vb
 
 extern "C" {
