@@ -531,7 +531,8 @@ template <typename R> static int bc_fill(vb_handle h, R* P, cudaStream_t s) {
     return VB_OK;
 }
 
-// split con2prim by default where it measured faster (3D)
+// split con2prim by default in 3D, where the stencil kernel then runs without
+// holding its registers through the divergent Newton (measured faster there)
 static int default_split(const vb_solver* h) { return h->dims == 3 ? 1 : 0; }
 
 template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s) {
