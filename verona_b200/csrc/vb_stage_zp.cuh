@@ -9,6 +9,13 @@
 // written on float2 lanes; reciprocal, square root, min/max and selects stay
 // per lane. Each barrier of the plane loop now serves two planes.
 //
+// Staging (TMA form, the default): every plane of the state, all five
+// variables with the 3-cell x/y halo of the CTA's column tile, arrives as one
+// TMA tile into a ring of six plane slots; the z window, the x/y stencils and
+// the halo reconstructions all read the ring. The other form loads the
+// thread's own column into a private z window and brings the x/y halo of each
+// pair of planes by 4-byte asynchronous copies into an interleaved buffer.
+//
 // Arithmetic differs from the scalar FP32 kernel only in rounding (packed
 // fma contraction written out by hand, 1/6 folded into the WENOZ stencil
 // weights, C^2 formed without the square root and re-square, approximate
