@@ -62,6 +62,8 @@ template <typename R, int TX, int TY> struct TmaTile2 {
     }
 };
 constexpr uint32_t TILE_MAX_POLLS = 1u << 22;  // bounded wait for the TMA tile
+static_assert(TmaTile2<double, 32, 8>::BXW >= 32 + 6 && (TmaTile2<double, 32, 8>::BXW * 8) % 16 == 0, "box row");
+static_assert(TmaTile2<float, 32, 8>::BXW >= 32 + 6 && (TmaTile2<float, 32, 8>::BXW * 4) % 16 == 0, "box row");
 
 // tensor map of a 2D state array for the TMA form of k_stage: dims (x, y,
 // variable) with byte strides (sy, vs) x element size; the box is TmaTile2's
@@ -461,7 +463,7 @@ cudaError_t launch_stage(int dims, int rec, int rs, const StageParams& p, const 
 // coalesced per variable.
 
 // dense padded cell c (x fastest, rows of n[0] cells) -> index in the pitched SoA arrays
-__device__ __forceinline__ long long soa_index(const Grid& g, long long c) {
+__host__ __device__ __forceinline__ long long soa_index(const Grid& g, long long c) {
     if (g.sy == g.n[0]) return c;
     const long long row = c / g.n[0];
     return (c - row * g.n[0]) + g.sy * row;  // sz == sy * n[1]: rows of every plane are consecutive

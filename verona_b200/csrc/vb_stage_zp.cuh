@@ -265,6 +265,12 @@ template <int TX, int TY> struct ZpTmaGeom {
         return 128 + 4 * (size_t)ZR * SLOTF + sizeof(float2) * NV * (size_t)(2 * G::FN + G::QXN) + 8 * ZR;
     }
 };
+// the TMA rules and the residency the launch bound assumes (2 CTAs per SM)
+static_assert(ZpTmaGeom<32, 8>::BXW >= 32 + 6 && (ZpTmaGeom<32, 8>::BXW * 4) % 16 == 0, "box row");
+static_assert((32 * 4) % 16 == 0, "box x start 32 * blockIdx.x is 16-byte aligned");
+static_assert(ZpTmaGeom<32, 8>::SLOTF * 4 % 128 == 0 && ZpTmaGeom<32, 8>::BOX_BYTES <= ZpTmaGeom<32, 8>::SLOTF * 4,
+              "ring slots hold one box and stay 128-byte aligned");
+static_assert(2 * (ZpTmaGeom<32, 8>::smem_bytes() + 1024) <= 228 * 1024, "two CTAs per SM");
 constexpr uint32_t ZP_MAX_POLLS = 1u << 22;  // bounded waits for a TMA plane
 
 // What a pair stage kernel leaves behind: con2prim done in the kernel (fused),
