@@ -226,6 +226,32 @@ def fp32_roofline(cells, stencil_ms, pair_stencil):
             "peak_kind": "measured in this run: cuBLAS SGEMM 8192^3 (torch, TF32 off)"}
 
 
+MLP_FLOP_PER_CELL = 2 * (4 * 64 + 64 * 64 + 64 * 64 + 64 * 1)  # one inference of the 4-64-64-64-1 network
+
+
+def tensor_roofline(cells, stage_ms, stencil_ms, learned_fused):
+    """Tensor-core roofline of the network inside the fused learned con2prim
+    kernel: algorithmic MLP FLOPs per cell (17,024) times the cells of one
+    stage launch over that kernel's live time (the stage group's time minus
+    the stencil's), against the sustained BF16 peak. The kernel also forms U
+    and runs the W Newton, and is bound by latency, not by the tensor cores."""
+    try:
+        c2p_ms = stage_ms - stencil_ms
+        if not learned_fused or not (stencil_ms > 0 and c2p_ms > 0):
+            return None
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peak, kind = float(json.load(f)["bf16_tflops_sustained"]), "measured (sustained)"
+        except Exception:
+            peak, kind = 1400.0, "fallback (sustained)"
+        ach = MLP_FLOP_PER_CELL * cells / (c2p_ms / 1e3) / 1e12
+        return {"bound": "tensor", "kernel": "k_c2p_learned (network part)", "achieved": ach, "peak": peak,
+                "unit": "TFLOP/s", "frac": ach / peak, "flop_per_cell": MLP_FLOP_PER_CELL,
+                "kernel_ms_per_launch": c2p_ms, "peak_kind": kind}
+    except Exception:
+        return None
+
+
 def fp32_gemm_tflops():
     """FP32 denominator of the stencil's compute roofline: cuBLAS SGEMM 8192^3
     on the CUDA cores (TF32 off), best of 3 after one warm-up."""
@@ -515,6 +541,8 @@ def run_ours(args, rank, world, dist):
                      "stage_ms_per_launch": stage_ms_per_launch},
         "roofline_fp32": fp32_roofline(cells, stencil_ms, learned_ok and args.learned_form == "fused"
                                        and args.stencil == "pairs"),
+        "roofline_tensor": tensor_roofline(cells, stage_ms_per_launch, stencil_ms,
+                                           learned_ok and args.learned_form == "fused"),
         "gpu_launches": launches,
         "clocks": clk.summary,
         "e2e": e2e,

@@ -25,3 +25,16 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"]
     assert d["e2e"]["value"] == d["value"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_tensor_roofline_of_the_learned_kernel():
+    sys.path.insert(0, ROOT)
+    import bench
+
+    r = bench.tensor_roofline(512**3, 16.1, 8.6, True)
+    assert r["bound"] == "tensor" and r["flop_per_cell"] == 17024
+    assert abs(r["kernel_ms_per_launch"] - 7.5) < 1e-9
+    assert abs(r["achieved"] - 17024 * 512**3 / 7.5e-3 / 1e12) < 1e-6
+    assert 0 < r["frac"] < 1
+    assert bench.tensor_roofline(512**3, 16.1, 8.6, False) is None
+    assert bench.tensor_roofline(512**3, 8.0, 8.6, True) is None
