@@ -114,3 +114,39 @@ def test_default_ic_is_the_examples():
     assert _lib.lib().vb_default_ic(2, 1, C.byref(ic)) == 0
     assert tuple(ic.box)[:2] == (800.0, 200.0) and ic.r_eng == 2.0 and ic.engine_rho == 1e-3
     assert _lib.lib().vb_default_ic(3, 5, C.byref(ic)) == -1  # VB_ERR_ARG
+
+
+def test_struct_layouts_match_the_ctypes_mirrors(tmp_path):
+    """Every POD struct of the header has the size and field offsets of its
+    ctypes mirror (and so of the Julia structs written after the same layout):
+    a C program built by gcc prints them with sizeof / offsetof."""
+    import shutil
+
+    from verona_b200 import _lib
+    from verona_b200.batch import BatchProblem
+
+    gcc = shutil.which("gcc") or shutil.which("cc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    mirrors = {"vb_options": _lib.VBOptions, "vb_tuning": _lib.VBTuning, "vb_ic_params": _lib.VBIcParams,
+               "vb_batch_problem": BatchProblem}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "verona_b200.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'    printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'    printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = str(tmp_path / "layout")
+    r = subprocess.run([gcc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", exe],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = {}
+    for line in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.splitlines():
+        cname, field, val = line.split()
+        got[(cname, field)] = int(val)
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
