@@ -48,8 +48,9 @@ template <int DIM, int TX, int TY, int TZ> struct TileGeom {
 
 // TMA form of the 2D tile: one box of the tile with its 3-cell halo on both
 // axes, every variable, [NV][TY + 6][BXW] (x fastest). The box starts at
-// x = x0 - 3 = TX * blockIdx.x, 16-byte aligned for TX a multiple of 4, and
-// is TX + 6 cells rounded up to a 16-byte row wide.
+// x = x0 - 3 = TX * blockIdx.x, 16-byte aligned when TX times the element
+// size is a multiple of 16, and is TX + 6 cells rounded up to a 16-byte row
+// wide.
 template <typename R, int TX, int TY> struct TmaTile2 {
     static constexpr int NV = 4;
     static constexpr int BXW = (TX + 6 + 16 / (int)sizeof(R) - 1) / (16 / (int)sizeof(R)) * (16 / (int)sizeof(R));
