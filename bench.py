@@ -47,6 +47,11 @@ def parse():
     ap.add_argument("--n", type=int, default=512, help="interior cells per axis")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-guess-compare", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip configs 1, 2, 3 and 5 next to the headline")
+    ap.add_argument("--config2-steps", type=int, default=200,
+                    help="steps of the 2D jet (config 2: 200)")
     ap.add_argument("--path", default="both", choices=["both", "fast", "fp64"],
                     help="fp64: time only the plain FP64 path (profiling runs)")
     ap.add_argument("--guess", default="auto", choices=["auto", "learned", "previous"],
@@ -100,12 +105,12 @@ def device_ic(n, seed):
     return P
 
 
-def make_solver(n, precision, guess):
+def make_solver(n, precision, guess, stats=0):
     from verona_b200 import Solver
 
     dx = 1.0 / n
     s = Solver(3, (n, n, n), GAMMA, (dx, dx, dx), recon="wenoz", riemann="hllc", rk=3, precision=precision,
-               guess=guess, n_iter=50, tol=1e-12, floor=1e-8)
+               guess=guess, n_iter=50, tol=1e-12, floor=1e-8, stats=stats)
     s.set_boundary(0, 2, nozzle(n))
     return s
 
@@ -186,6 +191,53 @@ def timed_steps(s, dt, warmup, steps, dist=None):
     s.profile(False)
     timed_steps.stencil_ms = stencil_ms
     return ms, stage_ms, stage_launches, launches
+
+
+def guess_comparison(n, P0, dt, W, K, dist, learned, stencil_ms_learned, stage_ms_learned, ms_learned):
+    """The learned guess against the method without it, the previous-state
+    warm start of the reference's con2prim (src/3dim/structs.jl:277-287), on
+    the same FP32-bulk workload: the previous-guess path timed like the
+    headline (its stencil and its con2prim kernel timed apart by the library's
+    profiling events), then both guesses run again with iteration statistics
+    (W steps, counters reset, 3 steps) for Newton iterations and fallbacks per
+    cell solve."""
+    import torch
+
+    from verona_b200 import mlp
+
+    out = {}
+    s = make_solver(n, "fp32", "previous")
+    s.load_prims(P0)
+    ms, st_ms, st_l, _ = timed_steps(s, dt, W, K, dist)
+    sten = timed_steps.stencil_ms / max(st_l, 1)
+    out["previous"] = {"ms_per_step": ms / K, "value": n**3 * K / (ms / 1e3), "stencil_ms_per_stage": sten,
+                       "c2p_ms_per_stage": st_ms / max(st_l, 1) - sten,
+                       "c2p_kernel": "k_c2p (the reference cascade from the previous primitive state)"}
+    s.close()
+    if learned:
+        out["learned"] = {"ms_per_step": ms_learned / K, "value": n**3 * K / (ms_learned / 1e3),
+                          "stencil_ms_per_stage": stencil_ms_learned,
+                          "c2p_ms_per_stage": stage_ms_learned - stencil_ms_learned,
+                          "c2p_kernel": "k_c2p_learned (U from the divergence, network guess, W Newton)"}
+    for guess in (("learned", "previous") if learned else ("previous",)):
+        s = make_solver(n, "fp32", guess, stats=1)
+        if guess == "learned":
+            mlp.attach(s)
+        s.load_prims(P0)
+        s.step(dt, W)
+        s.reset_counters()
+        s.step(dt, 3)
+        torch.cuda.synchronize()
+        c = s.counters()
+        s.close()
+        cells = max(int(c[3]), 1)
+        out[guess].update({"newton_iters_per_cell": float(c[2]) / cells, "fallbacks_per_cell": float(c[1]) / cells,
+                           "failures": int(c[0]), "cell_solves_counted": int(c[3])})
+    if learned:
+        out["c2p_speedup_learned_vs_previous"] = out["previous"]["c2p_ms_per_stage"] / out["learned"][
+            "c2p_ms_per_stage"]
+        out["step_speedup_learned_vs_previous"] = out["previous"]["ms_per_step"] / out["learned"]["ms_per_step"]
+    return out
 
 
 def l1_errors(a, b):
@@ -406,26 +458,51 @@ def run_ours(args, rank, world, dist):
                           "stage_ms_per_launch": st_ms / max(st_l, 1), "launches": ln}), flush=True)
         s.close()
         return
+    fp64_forms = {}
     if not args.no_fp64 and args.path == "both":
-        s = make_solver(n, "fp64", "previous")
-        s.load_prims(P0)
-        ms, st_ms, st_l, ln = timed_steps(s, dt, W, K, dist)
-        fp64 = {"value": cells * K / (ms / 1e3), "ms_per_step": ms / K, "stage_ms_per_launch": st_ms / max(st_l, 1)}
-        # FP64 roofline of the stage group (k_stage_zm<double> + k_c2p<double>):
-        # FP64 operations per cell (2 dfma + dadd + dmul, ncu counters of one
-        # RK-stage launch pair) over the group's live time, against DGEMM
-        flop = read_traffic("fp64_previous_stage_group_flop")
         peak64 = fp64_gemm_tflops()
-        if flop:
-            ach = flop * cells / (fp64["stage_ms_per_launch"] / 1e3) / 1e12
-            fp64["roofline"] = {"bound": "fp64", "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
-                                "frac": ach / peak64, "flop_per_cell": flop,
-                                "peak_kind": "measured in this run: cuBLAS DGEMM 8192^3 (torch)"}
-        P64 = s.store_prims()
-        torch.cuda.synchronize()
-        info["fp64_counters"] = s.counters().tolist()
-        s.close()
-        del s
+        hbm_peak, hbm_kind = read_peaks()
+        for form, contract in (("bitexact", 0), ("contracted", 1)):
+            s = make_solver(n, "fp64", "previous")
+            s.set_tuning(fp64_contract=contract)
+            s.load_prims(P0)
+            ms, st_ms, st_l, ln = timed_steps(s, dt, W, K, dist)
+            r = {"value": cells * K / (ms / 1e3), "ms_per_step": ms / K, "stage_ms_per_launch": st_ms / max(st_l, 1),
+                 "fma_contraction": bool(contract)}
+            # HBM roofline of the plain path: 560 B of compulsory traffic per
+            # zone-update of an FP64 SSP-RK3 step (14 passes of 5 FP64 arrays)
+            # at the measured step rate
+            ach_hbm = r["value"] * 560.0 / 1e9
+            r["roofline_hbm"] = {"bound": "hbm", "achieved": ach_hbm, "peak": hbm_peak, "unit": "GB/s",
+                                 "frac": ach_hbm / hbm_peak, "bytes_per_zone_update": 560.0, "peak_kind": hbm_kind}
+            # FP64 roofline of the stage group (k_stage_zm<double> + k_c2p<double>):
+            # FP64 operations per cell (2 dfma + dadd + dmul, ncu counters of one
+            # RK-stage launch pair) over the group's live time, against DGEMM
+            flop = read_traffic(f"fp64_previous_stage_group_flop{'_contracted' if contract else ''}")
+            if flop:
+                ach = flop * cells / (r["stage_ms_per_launch"] / 1e3) / 1e12
+                r["roofline"] = {"bound": "fp64", "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
+                                 "frac": ach / peak64, "flop_per_cell": flop,
+                                 "peak_kind": "measured in this run: cuBLAS DGEMM 8192^3 (torch)"}
+            Pout = s.store_prims()
+            torch.cuda.synchronize()
+            info[f"fp64_{form}_counters"] = s.counters().tolist()
+            s.close()
+            del s
+            fp64_forms[form] = (r, Pout)
+        P64 = fp64_forms["bitexact"][1]
+        # the contracted form against the bit-exact one (which equals the
+        # oracle bit for bit at small sizes): max difference per field over
+        # the field's max magnitude, on the full grid after W + K steps
+        Pc = fp64_forms["contracted"][1]
+        fp64_forms["contracted"][0]["max_rel_vs_bitexact"] = [
+            float((Pc[..., v] - P64[..., v]).abs().max() / P64[..., v].abs().max()) for v in range(5)]
+        del Pc
+        ok = max(fp64_forms["contracted"][0]["max_rel_vs_bitexact"]) <= 1e-10
+        fp64 = dict(fp64_forms["contracted" if ok else "bitexact"][0])
+        fp64["form"] = "contracted" if ok else "bitexact"
+        fp64["forms"] = {k: v[0] for k, v in fp64_forms.items()}
+        fp64_forms = {}
 
     # headline: FP32 bulk (+ learned guess when available)
     s = make_solver(n, "fp32", guess)
@@ -443,6 +520,11 @@ def run_ours(args, rank, world, dist):
     info["fast_counters"] = s.counters().tolist()
     err = l1_errors(Pf, P64) if fp64 else None
     del Pf
+    if fp64:
+        del P64
+    guesses = None
+    if args.path == "both" and not args.no_guess_compare:
+        guesses = guess_comparison(n, P0, dt, W, K, dist, learned_ok, stencil_ms, st_ms / max(st_l, 1), ms)
 
     t_tensor = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist is not None:
@@ -505,6 +587,11 @@ def run_ours(args, rank, world, dist):
                "d2h_bytes_per_step": nbytes / K,
                "note": f"one H2D of the FP64 AoS primitives, {K} steps, one D2H (the HARM_HLL call pattern)"}
     s.close()
+    del s
+    torch.cuda.empty_cache()
+    configs = None
+    if args.path == "both" and not args.no_configs:
+        configs = configs_measure(args, rank, world, dist)
 
     if rank != 0:
         return
@@ -530,7 +617,10 @@ def run_ours(args, rank, world, dist):
                        tma_tiles_active=tma_active),
         "fp64_plain": fp64,
         "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
+        "speedup_vs_fp64_denominator": (f"fp64_plain.forms.{fp64['form']}: the faster plain FP64 form within the "
+                                        "parity bar (1e-10 per field)") if fp64 else None,
         "l1_error_vs_fp64": err,
+        "guess_comparison": guesses,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic * cells if traffic else None, "peak_kind": peak_kind,
                      "per": "one RK-stage launch of the kernel group over the full grid",
@@ -547,6 +637,7 @@ def run_ours(args, rank, world, dist):
         "clocks": clk.summary,
         "e2e": e2e,
         "counters": info,
+        "configs": configs,
     }
     if dump is not None:
         line["dump"] = dump
@@ -559,7 +650,7 @@ def run_ours(args, rank, world, dist):
 BATCH_GAMMA = 5.0 / 3.0
 
 
-def run_batch(args, rank, world, dist):
+def batch_measure(K, W, rank, world, dist, e2e_on=True, single_on=True):
     """192 1D tubes (N in [256, 8192]) and 64 2D quadrant problems (side in
     [128, 1024]) from seed 42, MINMOD/PPM/WENOZ per problem, HLLC, SSP-RK3,
     FP32 bulk, gamma 5/3: K steps of every problem as one persistent launch."""
@@ -570,7 +661,6 @@ def run_batch(args, rank, world, dist):
     from verona_b200.autotune import tune_batch
     from verona_b200.batch import Batch, riemann_problems
 
-    K, W = args.steps, args.warmup
     opts = dict(riemann="hllc", rk=3, precision="fp32", n_iter=50, tol=1e-12, floor=1e-8)
     specs, prims = riemann_problems(42 + rank, gamma=BATCH_GAMMA)
     b = Batch(specs, BATCH_GAMMA, **opts)
@@ -601,8 +691,9 @@ def run_batch(args, rank, world, dist):
 
     # the same problems one grid at a time (a Solver per problem, its own launches)
     ks = max(1, min(K, 3))
+    single = None
     solvers = []
-    for spec, P in zip(specs, prims):
+    for spec, P in (zip(specs, prims) if single_on else ()):
         d = spec["dims"]
         dx = (spec["dx"],) if d == 1 else (spec["dx"], spec["dy"])
         s_ = Solver(d, spec["n"][:d], BATCH_GAMMA, dx, recon=spec["recon"], **opts)
@@ -616,13 +707,14 @@ def run_batch(args, rank, world, dist):
         s_.step(dt, ks)
     e1.record(stream)
     torch.cuda.synchronize()
-    single = cells * ks / (e0.elapsed_time(e1) / 1e3)
+    if single_on:
+        single = cells * ks / (e0.elapsed_time(e1) / 1e3)
     for s_, _ in solvers:
         s_.close()
 
     # e2e: host primitives in, K steps, host primitives out, through the public API
     e2e = None
-    if not args.no_e2e:
+    if e2e_on:
         host = [torch.from_numpy(np.ascontiguousarray(P.transpose(tuple(range(P.ndim - 1, -1, -1))))).pin_memory()
                 for P in prims]
         dev = [torch.empty(h.shape, dtype=torch.float64, device="cuda") for h in host]
@@ -641,8 +733,6 @@ def run_batch(args, rank, world, dist):
         e2e = {"value": world * cells * K / el, "unit": UNIT, "h2d_bytes_per_step": nbytes / K,
                "d2h_bytes_per_step": nbytes / K}
     b.close()
-    if rank != 0:
-        return
     peak, peak_kind = read_peaks()
     # algorithmic bytes per zone-update, FP32-bulk SSP-RK3: 6 passes of P (4 B)
     # and 8 of U (8 B) per variable; 3 variables in 1D, 4 in 2D
@@ -668,33 +758,39 @@ def run_batch(args, rank, world, dist):
         "clocks": clk.summary,
         "e2e": e2e,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
-def run_jet2d(args, rank, world, dist):
-    """2D relativistic jet 4096^2 (n x n with --n above 512), WENOZ + HLLC,
-    SSP-RK3, CFL 0.4, gamma 4/3: ambient rho = 1 (3 % seeded noise), p = 1e-3,
-    v = 0; nozzle of radius 32 cells on the x-lo face (rho 0.01, p 1e-3,
-    Lorentz factor 10 along +x), outflow elsewhere. FP64 (the plain method) and
-    the FP32-bulk form, each timed over K steps on the device; value = the
-    FP64 form's zone-updates/s summed over ranks (independent replicas)."""
+def run_batch(args, rank, world, dist):
+    line = batch_measure(args.steps, args.warmup, rank, world, dist, e2e_on=not args.no_e2e)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def jet2d_measure(n, K, W, rank, world, dist, planes="tma", forms=("fp64", "fp64c", "fp32")):
+    """2D relativistic jet n^2, WENOZ + HLLC, SSP-RK3, CFL 0.4, gamma 4/3:
+    ambient rho = 1 (3 % seeded noise), p = 1e-3, v = 0; nozzle of radius 32
+    cells on the x-lo face (rho 0.01, p 1e-3, Lorentz factor 10 along +x),
+    outflow elsewhere. Each form timed over K steps on the device after W:
+    fp64 (the plain method, the reference's rounding), fp64c (the plain
+    method with FMA contraction), fp32 (the FP32-bulk form)."""
     import math
 
     import torch
 
     from verona_b200 import Solver
 
-    n = args.n if args.n > 512 else 4096
-    K, W = args.steps, args.warmup
     dx = 1.0 / n
     dt = 0.4 / (2.0 * n)
-    tma = int(args.planes == "tma")
+    tma = int(planes == "tma")
+    hbm_peak, hbm_kind = read_peaks()
     res = {}
     with Clocks(torch.cuda.current_device()) as clk:
-        for prec in ("fp64", "fp32"):
+        for form in forms:
+            prec = "fp32" if form == "fp32" else "fp64"
             s = Solver(2, (n, n), GAMMA, (dx, dx), recon="wenoz", riemann="hllc", rk=3, precision=prec, n_iter=50,
                        tol=1e-12, floor=1e-8)
-            s.set_tuning(tma_tiles=tma)
+            s.set_tuning(tma_tiles=tma, fp64_contract=int(form == "fp64c"))
             tma_active = s.tma_tiles_active
             s.set_boundary(0, 2, [32.0, n / 2, 0.0, 0.01, 1e-3 / (GAMMA - 1), math.sqrt(99.0), 0.0, 0.0])
             s.init_prims("ambient", seed=7 + rank, noise=0.03, rho=1.0, u=1e-3 / (GAMMA - 1))
@@ -703,11 +799,25 @@ def run_jet2d(args, rank, world, dist):
             if dist is not None:
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
             c = s.counters()
-            res[prec] = {"value": world * n * n * K / (t.item() / 1e3), "ms_per_step": t.item() / K,
-                         "stage_ms_per_launch": st_ms / max(st_l, 1), "c2p_failures": int(c[0]),
-                         "tma_tiles_active": tma_active,
-                         "tma_timeouts": int(c[4])}
+            v = world * n * n * K / (t.item() / 1e3)
+            # compulsory traffic per zone-update of an SSP-RK3 step in 2D: 14
+            # passes of 4 arrays, P in FP32 for the FP32-bulk form (6 passes)
+            bpz = 6 * 4 * 4 + 8 * 4 * 8 if prec == "fp32" else 448.0
+            res[form] = {"value": v, "ms_per_step": t.item() / K, "stage_ms_per_launch": st_ms / max(st_l, 1),
+                         "c2p_failures": int(c[0]), "tma_tiles_active": tma_active, "tma_timeouts": int(c[4]),
+                         "roofline_hbm": {"achieved": v / world * bpz / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                                          "frac": v / world * bpz / 1e9 / hbm_peak, "bytes_per_zone_update": bpz,
+                                          "peak_kind": hbm_kind}}
+            s.close()
             del s
+    return res, clk.summary
+
+
+def run_jet2d(args, rank, world, dist):
+    """The 2D jet (config 2) alone: 4096^2 unless --n is above 512."""
+    n = args.n if args.n > 512 else 4096
+    K, W = args.steps, args.warmup
+    res, clocks = jet2d_measure(n, K, W, rank, world, dist, planes=args.planes)
     if rank != 0:
         return
     line = {
@@ -719,9 +829,135 @@ def run_jet2d(args, rank, world, dist):
                                "Gamma=10", "grid": [n, n], "tiles": args.planes,
                    "l2": "inputs larger than L2" if n * n * 4 * 8 > 126e6 else "inputs smaller than L2",
                    "parallelism": "replicas"},
-        "fp64": res["fp64"], "fp32_bulk": res["fp32"], "clocks": clk.summary,
+        "fp64": res["fp64"], "fp64_contracted": res["fp64c"], "fp32_bulk": res["fp32"], "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
+
+
+def config1_measure(rank):
+    """Config 1, Marti & Mueller problem 1 on N = 1024 cells to t = 0.4 (1024
+    steps, CFL 0.4, gamma 5/3): the reference's own 1D scheme
+    (Verona1D.HARM_HLL: MINMOD, HLL, midpoint RK2, no ghosts) on the GPU (one
+    persistent CTA runs every step) and as the oracle's C restatement on one
+    host core; and the configured form (MINMOD + HLLC, RK2, outflow ghosts)
+    through the ghosted 1D solver on the GPU and the oracle. zone-updates/s =
+    1024 cells x steps / time of the whole run."""
+    import numpy as np
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import mm1_ghosted, n_steps, shock_tube_1d
+    from oracle import oracle as O
+    from verona_b200 import Solver
+
+    g, N = 5.0 / 3.0, 1024
+    dx = 1.0 / N
+    dt = 0.4 * dx
+    steps, _ = n_steps(dt, 0.4)
+    out = {"cells": N, "steps": steps}
+    stream = torch.cuda.current_stream()
+
+    def gpu_time(s, P0):
+        s.load_prims(P0)
+        s.step(dt, 2)  # warm-up (module load, first launches)
+        s.load_prims(P0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.step(dt, steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    x, rho, u, ux = shock_tube_1d(N, gamma=g)
+    s = Solver(1, (N,), g, (dx,), nghost=0, recon="minmod", n_iter=50, tol=1e-12)
+    el = gpu_time(s, np.asfortranarray(np.stack([rho, u, ux])))
+    s.close()
+    t0 = time.perf_counter()
+    o = O.Solver1DRef(rho, u, ux, g, "minmod", 50, 1e-12)
+    o.step(dt, dx, steps)
+    el_cpu = time.perf_counter() - t0
+    out["reference_scheme_hll_rk2"] = {
+        "gpu": {"value": N * steps / el, "seconds": el, "kernel": "k_ref1d_steps (one persistent CTA)"},
+        "cpu_oracle": {"value": N * steps / el_cpu, "seconds": el_cpu, "cores": 1,
+                       "note": "the oracle's C restatement of Verona1D.HARM_HLL (the reference's CPU path)"}}
+    xg, P0 = mm1_ghosted(N, g)
+    s = Solver(1, (N,), g, (dx,), recon="minmod", riemann="hllc", rk=2, n_iter=50, tol=1e-12, floor=1e-10)
+    el = gpu_time(s, P0)
+    s.close()
+    t0 = time.perf_counter()
+    o = O.SolverND(1, (N,), P0, g, 1e-10, 50, 1e-12, O.MINMOD, O.HLLC, 2)
+    o.set_grid(dx)
+    o.step(dt, steps)
+    el_cpu = time.perf_counter() - t0
+    out["configured_minmod_hllc_rk2"] = {
+        "gpu": {"value": N * steps / el, "seconds": el, "kernel": "k_stage (box tiles), one launch per stage"},
+        "cpu_oracle": {"value": N * steps / el_cpu, "seconds": el_cpu, "cores": O.num_threads()}}
+    return out
+
+
+def config3_measure(n, K, W, rank, world, dist):
+    """Config 3's precision form on the 3D jet n^3 with PPM + HLLC (SSP-RK3,
+    gamma 4/3, nozzle radius 16 cells, Lorentz 10): the FP32-bulk form and
+    the plain FP64 path (FMA-contracted) over the same K steps after W from
+    the same state, with the L1 rho / p and max Lorentz-factor errors of the
+    FP32-bulk result against the FP64 one."""
+    import torch
+
+    from verona_b200 import Solver
+
+    dx = 1.0 / n
+    dt = dt_of(n)
+    P0 = device_ic(n, 42 + rank)
+    hbm_peak, hbm_kind = read_peaks()
+    res, outs = {}, {}
+    for prec in ("fp32", "fp64"):
+        s = Solver(3, (n, n, n), GAMMA, (dx, dx, dx), recon="ppm", riemann="hllc", rk=3, precision=prec,
+                   n_iter=50, tol=1e-12, floor=1e-8)
+        s.set_tuning(fp64_contract=int(prec == "fp64"))
+        s.set_boundary(0, 2, nozzle(n))
+        s.load_prims(P0)
+        ms, st_ms, st_l, _ = timed_steps(s, dt, W, K, dist)
+        v = world * n**3 * K / (ms / 1e3)
+        bpz = 440.0 if prec == "fp32" else 560.0
+        res[prec] = {"value": v, "ms_per_step": ms / K, "stage_ms_per_launch": st_ms / max(st_l, 1),
+                     "c2p_failures": int(s.counters()[0]),
+                     "roofline_hbm": {"achieved": v / world * bpz / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                                      "frac": v / world * bpz / 1e9 / hbm_peak, "bytes_per_zone_update": bpz,
+                                      "peak_kind": hbm_kind}}
+        outs[prec] = s.store_prims()
+        torch.cuda.synchronize()
+        s.close()
+        del s
+    del P0
+    res["l1_error_fp32_vs_fp64"] = l1_errors(outs["fp32"], outs["fp64"])
+    res["steps"] = K
+    res["speedup_fp32_vs_fp64"] = res["fp32"]["value"] / res["fp64"]["value"]
+    del outs
+    torch.cuda.empty_cache()
+    return res
+
+
+def configs_measure(args, rank, world, dist):
+    """Configs 1, 2, 3 and 5 of the task next to the headline (config 4)."""
+    import torch
+
+    out = {}
+    K, W = args.steps, args.warmup
+    out["config1_1d_shock_tube_1024"] = config1_measure(rank)
+    torch.cuda.empty_cache()
+    res, _ = jet2d_measure(4096, args.config2_steps, W, rank, world, dist)
+    out["config2_2d_jet_4096"] = dict(res, steps=args.config2_steps,
+                                      workload="2D jet 4096^2, WENOZ+HLLC, SSP-RK3, nozzle r=32 Gamma=10")
+    torch.cuda.empty_cache()
+    out["config3_3d_jet_512_ppm"] = dict(config3_measure(args.n, K, W, rank, world, dist),
+                                         workload=f"3D jet {args.n}^3, PPM+HLLC, SSP-RK3, nozzle r=16 Gamma=10")
+    torch.cuda.empty_cache()
+    b = batch_measure(K, W, rank, world, dist, e2e_on=False, single_on=False)
+    out["config5_batch_256"] = {k: b[k] for k in ("value", "ms_per_step", "roofline", "counters", "config")}
+    out["config5_batch_256"]["steps"] = K
+    torch.cuda.empty_cache()
+    return out
 
 
 def main():

@@ -4,7 +4,7 @@
  * Drop-in for the per-timestep update of Wesenheit/Verona's HARM_HLL solvers:
  *   Verona3D.HARM_HLL   src/3dim/algos.jl:203-362
  *   Verona2D.HARM_HLL   src/2dim/algos.jl:192-324
- *   Verona1D.HARM_HLL   src/1dim/algos.jl:169-426
+ *   Verona1D.HARM_HLL   src/1dim/algos.jl:58-315
  * The Julia host keeps grid/state construction, boundary choice, the time
  * loop and HDF5 output; it hands the library the device pointer of P.arr and
  * calls vb_step between dumps. Plain pointers, sizes and an opaque handle
@@ -106,7 +106,7 @@ int vb_default_options(vb_options* o);
  * nz = 1 in 2D). nghost = 3 selects the 2D/3D reference semantics and their
  * ghost-cell layout (src/{2,3}dim/algos.jl; also generic 1D); nghost = 0 with
  * dims = 1 selects the 1D reference solver on N = nx cells
- * (src/1dim/algos.jl:169-426). Replaces HARM_HLL's allocations
+ * (src/1dim/algos.jl:58-315). Replaces HARM_HLL's allocations
  * (src/3dim/algos.jl:221-257). */
 int vb_create(vb_handle* h, int dims, int nx, int ny, int nz, int nghost, const vb_options* o);
 int vb_destroy(vb_handle h);
@@ -215,14 +215,21 @@ int vb_reset_counters(vb_handle h, void* stream);
  * with its x/y halo, a ring of 6 planes per CTA; in 2D (both precisions) the
  * CTA's tile with its halo on both axes; 0 = staged by per-thread loads (3D:
  * the thread's own column, 4-byte asynchronous copies for the halo);
- * -1 = library default (1). Results are identical. */
+ * -1 = library default (1). Results are identical.
+ * fp64_contract (precision = VB_PREC_FP64): 1 = the stencil and con2prim
+ * kernels of the plain FP64 path built with FMA contraction (a * b + c
+ * rounded once), fewer FP64 instructions per cell; not bit-identical to the
+ * reference's rounding, held to the parity bar of 1e-10 per conserved field
+ * instead; 0 = the reference's rounding, bit-identical to its arithmetic
+ * (default). */
 typedef struct vb_tuning {
     int32_t split_con2prim;
     int32_t force_box;
     int32_t learned_fused;
     int32_t fp32_pairs;
     int32_t tma_tiles;
-    int32_t reserved[3];
+    int32_t fp64_contract;
+    int32_t reserved[2];
 } vb_tuning;
 int vb_set_tuning(vb_handle h, const vb_tuning* t);
 int vb_get_tuning(vb_handle h, vb_tuning* t);
@@ -242,9 +249,9 @@ int vb_memory_bytes(vb_handle h, uint64_t* bytes);
  * previous read, and resets them. */
 int vb_profile_enable(vb_handle h, int enable);
 int vb_profile_read(vb_handle h, double* stage_ms, int64_t* stage_launches, int64_t* all_launches);
-/* The same, with the part of the stage time spent in the stencil launcher
- * (for the learned guess: the stencil kernel alone; otherwise the stencil
- * and the con2prim kernel it launches). */
+/* The same, with the part of the stage time spent in the stencil kernel:
+ * the stencil alone where con2prim runs in a kernel of its own (the learned
+ * guess; the split 3D z-marching stages), else the fused stage kernel. */
 int vb_profile_read2(vb_handle h, double* stage_ms, double* stencil_ms, int64_t* stage_launches,
                      int64_t* all_launches);
 
@@ -391,6 +398,19 @@ int vb_batch_store_prims(vb_batch_handle b, int i, double* P_aos, void* stream);
 int vb_batch_step(vb_batch_handle b, int nsteps, void* stream);
 int vb_batch_get_time(vb_batch_handle b, int i, double* t);
 int vb_batch_get_counters(vb_batch_handle b, uint64_t* out /* VB_CNT_N */, void* stream); /* synchronises */
+/* Synchronises `stream` and reports the outcome of the steps before it:
+ * VB_ERR_TIMEOUT if a tile's bounded wait for the previous stage of its
+ * problem gave up (VB_CNT_TIMEOUT > 0; the batch state is then undefined:
+ * vb_batch_rollback or reload it), VB_ERR_STATE if work items were skipped as
+ * out of range, else VB_OK. The counters accumulate until
+ * vb_batch_reset_counters. No counterpart in the reference (its kernels have
+ * no waits). */
+int vb_batch_check(vb_batch_handle b, void* stream);
+/* Bound of a tile's wait for the previous stage of its problem, in polls of
+ * about 128 ns; 0 restores the default (2^24, a few seconds). Every wait ends
+ * by construction (the tiles waited for are held by running CTAs); a smaller
+ * bound only makes a stalled launch end sooner. */
+int vb_batch_set_wait_limit(vb_batch_handle b, uint32_t max_polls);
 int vb_batch_reset_counters(vb_batch_handle b, void* stream);
 /* tile variants of a precision (0 for an invalid precision) and their shapes */
 int vb_batch_num_variants(int precision);

@@ -50,6 +50,8 @@ def lib():
         L.or_prim2con.argtypes = [C.c_int, C.c_double, _dp, _dp]
         L.or_con2prim.argtypes = [C.c_int, C.c_double, C.c_int, C.c_double, _dp, _dp]
         L.or_con2prim.restype = C.c_int
+        L.or_lu4_swaps_take.argtypes = []
+        L.or_lu4_swaps_take.restype = C.c_longlong
         L.or1d_create.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double, C.c_int, C.c_int, C.c_double]
         L.or1d_create.restype = C.c_void_p
         L.or1d_step.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
@@ -111,6 +113,11 @@ def con2prim(dims: int, gamma: float, n_iter: int, tol: float, U, guess) -> tupl
     return P, r
 
 
+def lu4_swaps_take() -> int:
+    """Row swaps of the 2D con2prim's pivoted LU on this thread since the last call."""
+    return int(lib().or_lu4_swaps_take())
+
+
 def face_flux(dims: int, axis: int, riemann: int, gamma: float, PL, PR) -> np.ndarray:
     PL = np.ascontiguousarray(PL, dtype=np.float64)
     PR = np.ascontiguousarray(PR, dtype=np.float64)
@@ -120,7 +127,7 @@ def face_flux(dims: int, axis: int, riemann: int, gamma: float, PL, PR) -> np.nd
 
 
 class Solver1DRef:
-    """Verona1D.HARM_HLL (src/1dim/algos.jl:169-426): N cells, no ghosts."""
+    """Verona1D.HARM_HLL (src/1dim/algos.jl:58-315): N cells, no ghosts."""
 
     def __init__(self, rho, u, ux, gamma, rec, n_iter, tol):
         self.N = len(rho)

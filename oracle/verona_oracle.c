@@ -404,6 +404,16 @@ static int c2p_1d(double g, int n_iter, double tol, const double* U, double* P) 
     return it;
 }
 
+/* Row swaps made by lu_pivot4 on this thread since the last or_lu4_swaps_take
+ * (instrumentation for the tests that show the pivoting path runs; it does not
+ * touch the arithmetic). */
+static _Thread_local long long g_lu4_swaps = 0;
+long long or_lu4_swaps_take(void) {
+    long long n = g_lu4_swaps;
+    g_lu4_swaps = 0;
+    return n;
+}
+
 /* LU_dec_pivot!, src/2dim/structs.jl:121-208 (4x4, scaled partial pivoting,
  * explicit fma). Returns 0 on a row-wise singular matrix (the reference
  * throws there). */
@@ -430,6 +440,7 @@ static int lu_pivot4(double* A, double* t, double* x) {
             }
         }
         if (piv != k) {
+            ++g_lu4_swaps;
             for (int j = 1; j <= 4; ++j) {
                 double tmp = A[I4(k, j)];
                 A[I4(k, j)] = A[I4(piv, j)];
@@ -749,7 +760,7 @@ int or_con2prim(int dims, double g, int n_iter, double tol, const double* U, dou
 }
 
 /* ========================================================================== */
-/* 1D reference solver, src/1dim/algos.jl:169-426                             */
+/* 1D reference solver, src/1dim/algos.jl:58-315                             */
 /* ========================================================================== */
 struct or1d {
     int N;
@@ -801,7 +812,7 @@ or1d_t* or1d_create(int N, const double* rho, const double* u, const double* ux,
 }
 
 /* one stage: reconstruction into PR/PL, HLL fluxes F, update into Uout
- * (src/1dim/algos.jl:202-288 / :295-413) */
+ * (src/1dim/algos.jl:91-177 / :184-302) */
 static void stage_1dref(or1d_t* s, const double* P, const double* Ubase, double* Uout, double coef) {
     const int N = s->N;
     const double g = s->g;
@@ -1087,7 +1098,7 @@ void ornd_set_boundary(ornd_t* s, int face, int kind, const double* par, int np)
 
 /* Ghost fill at the start of a step. This is the on-device replacement of the
  * user boundary callback `TurnOff` (examples/Jet3D/HARM_jet_breakout.jl:131-158,
- * examples/Jet2D/HARM_jet_breakout.jl:278-293): first the decay of FIXED faces,
+ * examples/Jet2D/HARM_jet_breakout.jl:84-99): first the decay of FIXED faces,
  * then faces in the order y-lo, y-hi, z-lo, z-hi, x-lo, x-hi, each spanning the
  * full padded extent of the other axes. OUTFLOW copies the first interior
  * cell into the three ghost layers. NOZZLE holds a fixed inflow state inside

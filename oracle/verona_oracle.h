@@ -40,8 +40,11 @@ void or_prim2con(int dims, double gamma, const double* P, double* U);
 /* con2prim on one cell; returns the cascade stage that converged (3D) or the
  * Newton iteration count, negative on failure. P is the guess on entry. */
 int or_con2prim(int dims, double gamma, int n_iter, double tol, const double* U, double* P);
+/* row swaps of the 2D con2prim's pivoted LU (LU_dec_pivot!) made on the calling
+ * thread since the previous call; the count is reset */
+long long or_lu4_swaps_take(void);
 
-/* 1D reference solver (src/1dim/algos.jl:169-426): N cells, no ghosts ---- */
+/* 1D reference solver (src/1dim/algos.jl:58-315): N cells, no ghosts ---- */
 typedef struct or1d or1d_t;
 or1d_t* or1d_create(int N, const double* rho, const double* u, const double* ux,
                     double gamma, int rec, int n_iter, double tol);

@@ -152,3 +152,52 @@ def test_config5_batch_of_256_uneven_problems_fp32_against_fp64():
                                              np.nonzero(errs > 1e-5)[0].tolist()))
     assert len(outliers) <= 8 and all(specs[i]["dims"] == 1 for i in outliers), outliers
     assert np.median(errs) <= 1e-7 and np.delete(errs, outliers).max() <= 1e-5
+
+
+def test_jet_128_fp32_and_learned_against_the_oracle():
+    """The 3D jet at 128^3 (WENOZ + HLLC, SSP-RK3, nozzle radius 4 cells,
+    Lorentz 10, ambient with 3 % density noise), 5 steps, with the errors
+    taken directly against the C FP64 oracle run from the same initial state:
+    the plain FP64 path within 1e-10 per field, the FP32-bulk form and the
+    learned guess + FP32 bulk within L1 density 1e-5 (the precision form's
+    bar) and L1 pressure 1e-4."""
+    from helpers import per_field_rel
+    from oracle import oracle as O
+    from verona_b200 import Solver, mlp
+
+    g, n, steps = 4.0 / 3.0, 128, 5
+    dxs = (1.0 / n,) * 3
+    dt = 0.4 / (3.0 * n)
+    noz = nozzle_params(3, (n, n, n), 4.0, gamma=g)
+    got, P0 = {}, None
+    for prec, guess in (("fp64", "previous"), ("fp32", "previous"), ("fp32", "learned")):
+        s = Solver(3, (n, n, n), g, dxs, recon="wenoz", riemann="hllc", rk=3, precision=prec, guess=guess, n_iter=50,
+                   tol=1e-12, floor=1e-8)
+        if guess == "learned":
+            mlp.attach(s)
+        s.init_prims("ambient", rho=1.0, u=1e-3 / (g - 1), noise=0.03, seed=42)
+        if P0 is None:
+            P0 = s.prims()
+        s.set_boundary(0, 2, noz)
+        s.step(dt, steps)
+        got[(prec, guess)] = s.prims()
+        assert s.counters()[0] == 0
+        s.close()
+    o = O.SolverND(3, (n, n, n), P0, g, 1e-8, 50, 1e-12, O.WENOZ, O.HLLC, 3)
+    o.set_grid(*dxs)
+    o.set_boundary(0, O.BC_NOZZLE, noz)
+    o.step(dt, steps)
+    ref = o.prims()
+    e64 = per_field_rel(got[("fp64", "previous")], ref)
+    print("128^3 FP64 vs oracle: max rel per field", e64, "differing values:",
+          int(np.sum(got[("fp64", "previous")] != ref)))
+    assert max(e64) <= 1e-10
+    r = ref[:, 3:-3, 3:-3, 3:-3]
+    lr = np.sqrt(1 + (r[2:] ** 2).sum(0))
+    for key in (("fp32", "previous"), ("fp32", "learned")):
+        a = got[key][:, 3:-3, 3:-3, 3:-3]
+        l1r = float(np.mean(np.abs(a[0] - r[0])) / np.mean(np.abs(r[0])))
+        l1p = float(np.mean(np.abs(a[1] - r[1])) / np.mean(np.abs(r[1])))
+        dl = float(np.max(np.abs(np.sqrt(1 + (a[2:] ** 2).sum(0)) - lr)))
+        print("128^3 %s + %s guess vs oracle: L1 rho %.3e L1 p %.3e max |dGamma| %.3e" % (key + (l1r, l1p, dl)))
+        assert np.all(np.isfinite(a)) and l1r <= 1e-5 and l1p <= 1e-4

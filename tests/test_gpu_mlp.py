@@ -241,9 +241,12 @@ def test_w_newton_recovers_the_primitive_state():
     U = mlp.prim2con_torch(P, G)
     lor = torch.sqrt(1 + P[2] ** 2 + P[3] ** 2 + P[4] ** 2)
     W = (P[0] + G * P[1]) * lor**2
-    for W0, slack in ((W * (1 + 1e-3), 1.0), (U[0] - U[1], 10.0)):
-        R, it, fb = mlp.c2p_w(U, W0, G)
+    # third form: max_newton = 0, the bracketed phase alone solves every cell
+    for W0, slack, mn in ((W * (1 + 1e-3), 1.0, 8), (U[0] - U[1], 10.0, 8), (W * (1 + 1e-3), 10.0, 0)):
+        R, it, fb = mlp.c2p_w(U, W0, G, max_newton=mn, max_bracket=400)
         assert (it > 0).all()
+        if mn == 0:
+            assert bool(fb.bool().all())
         er = ((R[0] - P[0]).abs() / P[0] / (slack * 1e-10 * lor**2)).max().item()
         ev = ((R[2:5] - P[2:5]).abs() / (slack * 1e-10 * lor**3)).max().item()
         eu = ((R[1] - P[1].clamp(min=1e-8)).abs() / (slack * 1e-9 * W + 2e-8)).max().item()

@@ -409,3 +409,155 @@ def test_diverging_reference_newton_is_counted_as_failure():
     c = s.counters()
     print("non-finite values", bad, "counters", c.tolist())
     assert bad > 0 and c[0] > 0
+
+
+@pytest.mark.parametrize("rec", ["minmod", "ppm", "wenoz"])
+def test_hllc_keeps_an_isolated_contact_exact_on_the_gpu(oracle, rec):
+    """GPU twin of the HLLC known answer: the stationary contact stays exactly
+    two-valued (p and v exactly unchanged) after 40 SSP-RK3 steps of the
+    ghosted 1D solver, bit-identical to the oracle."""
+    from helpers import contact_1d
+    from verona_b200 import Solver
+
+    g = 5.0 / 3.0
+    N = 64
+    P0 = contact_1d(N, gamma=g)
+    s = Solver(1, (N,), g, (1.0 / N,), recon=rec, riemann="hllc", rk=3, n_iter=50, tol=1e-12, floor=1e-10)
+    s.load_prims(P0)
+    s.step(0.4 / N, 40)
+    got = s.prims()
+    o = oracle.SolverND(1, (N,), P0, g, 1e-10, 50, 1e-12, oracle.RECON[rec], oracle.HLLC, 3)
+    o.set_grid(1.0 / N)
+    o.step(0.4 / N, 40)
+    np.testing.assert_array_equal(got, o.prims())
+    Q = got[:, 3:-3]
+    assert np.max(np.minimum(np.abs(Q[0] - 10.0), np.abs(Q[0] - 1.0))) == 0.0
+    assert np.all(Q[1] * (g - 1) == 1.0) and np.all(Q[2] == 0.0)
+
+
+@pytest.mark.parametrize("rec", ["minmod", "ppm", "wenoz"])
+def test_hllc_shock_tube_matches_oracle_and_exact_solution(oracle, rec):
+    """Marti & Mueller problem 1 (config 1's states) through the ghosted 1D
+    solver with HLLC + SSP-RK3 at N = 512 to t = 0.4: bit-identical to the
+    oracle, and within the oracle's L1 density error of the exact solution."""
+    from oracle import exact_riemann as ER
+
+    from helpers import mm1_ghosted
+    from verona_b200 import Solver
+
+    g = 5.0 / 3.0
+    N = 512
+    x, P0 = mm1_ghosted(N, g)
+    dt = 0.4 / N
+    n, t = n_steps(dt, 0.4)
+    s = Solver(1, (N,), g, (1.0 / N,), recon=rec, riemann="hllc", rk=3, n_iter=50, tol=1e-12, floor=1e-10)
+    s.load_prims(P0)
+    s.step(dt, n)
+    got = s.prims()
+    o = oracle.SolverND(1, (N,), P0, g, 1e-10, 50, 1e-12, oracle.RECON[rec], oracle.HLLC, 3)
+    o.set_grid(1.0 / N)
+    o.step(dt, n)
+    ref = o.prims()
+    assert max(per_field_rel(got, ref)) <= TOL
+    print(f"{rec}: {int(np.sum(got != ref))} of {got.size} values differ from the oracle")
+    ex = ER.solve(10.0, 13.33, 0.0, 1.0, 1e-6, 0.0, g, x, t)
+    assert float(np.mean(np.abs(got[0, 3:-3] - ex[0]))) < 0.05
+
+
+@pytest.mark.parametrize("rec", [0, 1, 2])
+@pytest.mark.parametrize("rs", [0, 1])
+@pytest.mark.parametrize("variant", ["fused", "split", "box"])
+def test_fp64_contracted_path_within_parity_bar(oracle, rec, rs, variant):
+    """The plain FP64 path with FMA contraction (vb_tuning.fp64_contract):
+    not bit-identical to the reference's rounding, but within the parity bar
+    of 1e-10 per conserved field of the oracle after 6 SSP-RK3 steps of a jet
+    on the z-marching grid (70 cells in z: two z-ranges, the second partial),
+    for every kernel variant."""
+    from verona_b200 import Solver
+
+    g = 4.0 / 3.0
+    n = (32, 16, 70)
+    P0 = jet_ic(3, n, gamma=g, noise=0.03, seed=23)
+    dxs = [1.0 / 32] * 3
+    dt = 0.4 / sum(1.0 / d for d in dxs)
+    noz = nozzle_params(3, n, 5.0, gamma=g)
+    s = Solver(3, n, g, dxs, recon=rec, riemann=rs, rk=3, n_iter=50, tol=1e-12, floor=1e-8)
+    s.set_tuning(split_con2prim=int(variant == "split"), force_box=int(variant == "box"), fp64_contract=1)
+    assert s.get_tuning()["fp64_contract"] == 1
+    s.set_boundary(0, 2, noz)
+    s.load_prims(P0)
+    s.step(dt, 6)
+    o = oracle.SolverND(3, n, P0, g, 1e-8, 50, 1e-12, rec, rs, 3)
+    o.set_grid(*dxs)
+    o.set_boundary(0, oracle.BC_NOZZLE, noz)
+    o.step(dt, 6)
+    got, ref = s.prims(), o.prims()
+    eU = per_field_rel(s.cons(), o.cons())
+    eP = per_field_rel(got, ref)
+    print("contracted", rec, rs, variant, "U", max(eU), "P", max(eP), "differing", int(np.sum(got != ref)))
+    assert max(eU) <= TOL and max(eP) <= TOL
+    assert np.sum(got != ref) > 0  # the contracted kernels did run
+
+
+@pytest.mark.parametrize("dims", [1, 2])
+@pytest.mark.parametrize("contract", [0, 1])
+def test_fp64_1d_2d_inflow_within_parity_bar(oracle, dims, contract):
+    """The FP64 box-tile kernels of the 1D and 2D grids (the 2D tiles by TMA),
+    WENOZ + HLLC + SSP-RK3 with an inflow (2D: the nozzle; 1D: FIXED x-lo
+    ghosts holding u^x = 3), against the oracle after 10 steps: bit-identical
+    with the reference's rounding, within 1e-10 per field with FMA
+    contraction (vb_tuning.fp64_contract)."""
+    from verona_b200 import Solver
+
+    g = 4.0 / 3.0
+    n = (200, 1, 1) if dims == 1 else (64, 48, 1)
+    P0 = jet_ic(dims, n, gamma=g, noise=0.03, seed=24)
+    dxs = [1.0 / n[0]] * dims
+    dt = 0.4 / sum(1.0 / d for d in dxs)
+    s = Solver(dims, n[:dims], g, dxs, recon="wenoz", riemann="hllc", rk=3, n_iter=50, tol=1e-12, floor=1e-8)
+    s.set_tuning(fp64_contract=contract)
+    o = oracle.SolverND(dims, n[:dims], P0, g, 1e-8, 50, 1e-12, oracle.WENOZ, oracle.HLLC, 3)
+    o.set_grid(*(dxs + [1.0] * (3 - dims)))
+    if dims == 2:
+        noz = nozzle_params(2, n, 4.0, gamma=g)
+        s.set_boundary(0, 2, noz)
+        o.set_boundary(0, oracle.BC_NOZZLE, noz)
+    else:
+        P0[2, :3] = 3.0  # an inflow into the tube through the x-lo ghosts
+        s.set_boundary(0, 1)
+        o.set_boundary(0, oracle.BC_FIXED, (-1.0, 0.0, 0.0, 1.0))
+    s.load_prims(P0)
+    s.step(dt, 10)
+    o.step(dt, 10)
+    got, ref = s.prims(), o.prims()
+    eU = per_field_rel(s.cons(), o.cons())
+    eP = per_field_rel(got, ref)
+    print("inflow", dims, "contract", contract, "U", max(eU), "P", max(eP), "differing", int(np.sum(got != ref)),
+          "max |P|", float(np.max(np.abs(got))))
+    if contract == 0:
+        np.testing.assert_array_equal(got, ref)
+    assert max(eU) <= TOL and max(eP) <= TOL
+
+
+@pytest.mark.parametrize("rec", ["minmod", "wenoz"])
+def test_fp64_contracted_1d_shock_tube_within_parity_bar(oracle, rec):
+    """Marti & Mueller problem 1 through the ghosted 1D solver with the
+    FMA-contracted FP64 kernels, HLLC + SSP-RK3, N = 256, 60 steps: within
+    1e-10 per field of the oracle."""
+    from helpers import mm1_ghosted
+    from verona_b200 import Solver
+
+    g = 5.0 / 3.0
+    N = 256
+    _, P0 = mm1_ghosted(N, g)
+    s = Solver(1, (N,), g, (1.0 / N,), recon=rec, riemann="hllc", rk=3, n_iter=50, tol=1e-12, floor=1e-10)
+    s.set_tuning(fp64_contract=1)
+    s.load_prims(P0)
+    s.step(0.4 / N, 60)
+    o = oracle.SolverND(1, (N,), P0, g, 1e-10, 50, 1e-12, oracle.RECON[rec], oracle.HLLC, 3)
+    o.set_grid(1.0 / N)
+    o.step(0.4 / N, 60)
+    got, ref = s.prims(), o.prims()
+    e = per_field_rel(got, ref)
+    print("contracted mm1", rec, e, "differing", int(np.sum(got != ref)))
+    assert max(e) <= TOL

@@ -91,3 +91,60 @@ def test_point_con2prim_bitwise(oracle, dims):
         ref, r = oracle.con2prim(dims, g, 50, 1e-12, U[:, i], guess[:, i])
         same = (got[:, i] == ref) | (np.isnan(got[:, i]) & np.isnan(ref))
         assert same.all() and ret[i] == r, (i, got[:, i], ref, ret[i], r)
+
+
+def _gpu_con2prim(dims, g, n_iter, U, guess):
+    import torch
+
+    from verona_b200 import _lib as L
+
+    n = U.shape[1]
+    dU, dP = _dev(U), _dev(guess)
+    dr = torch.zeros(n, dtype=torch.int32, device="cuda")
+    L.check(L.lib().vb_point_con2prim(dims, g, n_iter, 1e-12, C.c_void_p(dU.data_ptr()), C.c_void_p(dP.data_ptr()),
+                                      C.c_void_p(dr.data_ptr()), n, None))
+    return dP.cpu().numpy(), dr.cpu().numpy()
+
+
+def test_point_con2prim_every_cascade_stage_bitwise(oracle):
+    """The 3D cascade driven into each of its stages (1DW, Noble 2D with line
+    search, 5D primitive Newton, bisection) and its failure exit
+    (src/3dim/structs.jl:258-620): the GPU returns the same stage and the same
+    bits as the oracle in every cell, and every stage occurs."""
+    from collections import Counter
+
+    from helpers import c2p_cascade_cases
+
+    g = 4.0 / 3.0
+    hist = Counter()
+    for n_iter, P, guess in c2p_cascade_cases(g):
+        U = np.stack([oracle.prim2con(3, g, P[:, i]) for i in range(P.shape[1])], axis=1)
+        got, ret = _gpu_con2prim(3, g, n_iter, U, guess)
+        for i in range(P.shape[1]):
+            ref, r = oracle.con2prim(3, g, n_iter, 1e-12, U[:, i], guess[:, i])
+            same = (got[:, i] == ref) | (np.isnan(got[:, i]) & np.isnan(ref))
+            assert same.all() and ret[i] == r, (n_iter, i, got[:, i], ref, ret[i], r)
+            hist[r] += 1
+    print("stages:", dict(sorted(hist.items())))
+    for stage in (1, 2, 3, 4, -1):
+        assert hist[stage] >= 10, (stage, dict(hist))
+
+
+def test_point_con2prim_2d_pivoting_bitwise(oracle):
+    """The 2D con2prim's scaled partial pivoting (LU_dec_pivot!,
+    src/2dim/structs.jl:121-208) on states where it swaps rows in most cells:
+    bitwise against the oracle, iteration counts included."""
+    from helpers import c2p_pivot_cases
+
+    g = 4.0 / 3.0
+    P, guess = c2p_pivot_cases(g)
+    U = np.stack([oracle.prim2con(2, g, P[:, i]) for i in range(P.shape[1])], axis=1)
+    got, ret = _gpu_con2prim(2, g, 50, U, guess)
+    with_swaps = 0
+    for i in range(P.shape[1]):
+        oracle.lu4_swaps_take()
+        ref, r = oracle.con2prim(2, g, 50, 1e-12, U[:, i], guess[:, i])
+        with_swaps += oracle.lu4_swaps_take() > 0
+        same = (got[:, i] == ref) | (np.isnan(got[:, i]) & np.isnan(ref))
+        assert same.all() and ret[i] == r, (i, got[:, i], ref, ret[i], r)
+    assert with_swaps >= P.shape[1] // 3, with_swaps

@@ -1,7 +1,10 @@
-"""Index maps of the pitched SoA layout, checked on the CPU: tests/index_check.cu
-includes the kernels' header, is built by nvcc as a host program and compares
-CellMap (interior cell -> pitched index, multiply-high division) and soa_index
-(dense padded cell -> pitched index) with plain loops."""
+"""Device helpers checked on the CPU: each check includes the kernels' headers,
+is built by nvcc as a host program and prints "ok".
+- tests/index_check.cu: the index maps of the pitched SoA layout, CellMap
+  (interior cell -> pitched index, multiply-high division) and soa_index
+  (dense padded cell -> pitched index), against plain loops.
+- tests/c2pw_check.cu: the W Newton of the learned guess (c2p_w) and its
+  bracketed fallback, against P -> U -> P round trips."""
 import os
 import shutil
 import subprocess
@@ -18,10 +21,9 @@ def _nvcc():
     return None
 
 
-@pytest.mark.skipif(_nvcc() is None, reason="nvcc not found")
-def test_pitched_index_maps_match_plain_loops(tmp_path):
-    exe = str(tmp_path / "index_check")
-    src = os.path.join(ROOT, "tests", "index_check.cu")
+def _build_and_run(tmp_path, name):
+    exe = str(tmp_path / name)
+    src = os.path.join(ROOT, "tests", name + ".cu")
     inc = ["-I", os.path.join(ROOT, "verona_b200", "csrc"), "-I", os.path.join(ROOT, "include")]
     r = subprocess.run([_nvcc(), "-std=c++17", "-O1", "--expt-relaxed-constexpr", "-gencode",
                         "arch=compute_100a,code=sm_100a", *inc, src, "-o", exe], capture_output=True, text=True,
@@ -29,3 +31,16 @@ def test_pitched_index_maps_match_plain_loops(tmp_path):
     assert r.returncode == 0, r.stderr[-3000:]
     out = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0 and out.stdout.strip() == "ok", out.stdout + out.stderr
+
+
+@pytest.mark.skipif(_nvcc() is None, reason="nvcc not found")
+def test_pitched_index_maps_match_plain_loops(tmp_path):
+    _build_and_run(tmp_path, "index_check")
+
+
+@pytest.mark.skipif(_nvcc() is None, reason="nvcc not found")
+def test_w_newton_and_its_bracketed_fallback_recover_the_state(tmp_path):
+    """The bracketed phase alone (max_newton = 0) must solve every cell; an
+    earlier form evaluated its residual with a loop counter in place of
+    (gamma - 1) / gamma and missed the root by up to 5e-4 of U."""
+    _build_and_run(tmp_path, "c2pw_check")

@@ -179,3 +179,94 @@ def test_ic_star_jet_follows_the_examples():
     assert ux[0, 15, 15] == 0.0 and abs(rho[0, 15, 15] / (2.5e-2 * (100 / 7.5) ** 2) - 1) < 0.2
     assert np.all(rho[-1] == 1e-4)  # X = 480 is outside R_max
     assert np.allclose(u[rho == 1e-4], 1e-9)
+
+
+def test_cascade_inputs_reach_every_con2prim_stage(oracle):
+    """The inputs of the GPU cascade test reach every stage of the 3D
+    con2prim (1DW, Noble 2D, 5D Newton, bisection) and its failure exit, so
+    the bitwise comparison there covers each stage's code."""
+    from collections import Counter
+
+    from helpers import c2p_cascade_cases
+
+    g = 4.0 / 3.0
+    hist = Counter()
+    for n_iter, P, guess in c2p_cascade_cases(g):
+        for i in range(P.shape[1]):
+            U = oracle.prim2con(3, g, P[:, i])
+            _, r = oracle.con2prim(3, g, n_iter, 1e-12, U, guess[:, i])
+            hist[r] += 1
+    print(dict(sorted(hist.items())))
+    for stage in (1, 2, 3, 4, -1):
+        assert hist[stage] >= 10, (stage, dict(hist))
+
+
+def test_pivot_inputs_swap_rows_in_the_2d_lu(oracle):
+    """The inputs of the GPU pivoting test make the 2D con2prim's scaled
+    partial pivoting swap rows in at least a third of the cells."""
+    from helpers import c2p_pivot_cases
+
+    g = 4.0 / 3.0
+    P, guess = c2p_pivot_cases(g)
+    with_swaps = 0
+    for i in range(P.shape[1]):
+        U = oracle.prim2con(2, g, P[:, i])
+        oracle.lu4_swaps_take()
+        oracle.con2prim(2, g, 50, 1e-12, U, guess[:, i])
+        with_swaps += oracle.lu4_swaps_take() > 0
+    assert with_swaps >= P.shape[1] // 3, with_swaps
+
+
+@pytest.mark.parametrize("rec", ["minmod", "ppm", "wenoz"])
+def test_hllc_keeps_an_isolated_contact_exact(oracle, rec):
+    """Known answer of the HLLC solver (Mignone & Bodo 2005): a stationary
+    contact (equal p, v = 0, density jump) is an exact solution of the
+    scheme, so the density stays exactly two-valued and p, v exactly
+    unchanged after 40 SSP-RK3 steps; the HLL flux of the reference smears it
+    over several cells."""
+    from helpers import contact_1d
+
+    g = 5.0 / 3.0
+    N = 64
+    dev = {}
+    for rs in (oracle.HLL, oracle.HLLC):
+        s = oracle.SolverND(1, (N,), contact_1d(N, gamma=g), g, 1e-10, 50, 1e-12, oracle.RECON[rec], rs, 3)
+        s.set_grid(1.0 / N)
+        s.step(0.4 / N, 40)
+        Q = s.prims()[:, 3:-3]
+        dev[rs] = float(np.max(np.minimum(np.abs(Q[0] - 10.0), np.abs(Q[0] - 1.0))))
+        if rs == oracle.HLLC:
+            assert dev[rs] == 0.0
+            assert np.all(Q[1] * (g - 1) == 1.0) and np.all(Q[2] == 0.0)
+    assert dev[oracle.HLL] > 1.0, dev
+
+
+@pytest.mark.parametrize("rec", ["minmod", "ppm", "wenoz"])
+def test_hllc_converges_to_the_exact_solution_like_hll(oracle, rec):
+    """Marti & Mueller problem 1 through the ghosted 1D solver with SSP-RK3:
+    with HLLC the L1 density error against the exact solution falls with N at
+    least as HLL's does (within 5 % at every N)."""
+    from oracle import exact_riemann as ER
+
+    from helpers import mm1_ghosted
+
+    g = 5.0 / 3.0
+    errs = {}
+    for rs in (oracle.HLL, oracle.HLLC):
+        errs[rs] = []
+        for N in (128, 256, 512):
+            x, P = mm1_ghosted(N, g)
+            s = oracle.SolverND(1, (N,), P, g, 1e-10, 50, 1e-12, oracle.RECON[rec], rs, 3)
+            dt = 0.4 / N
+            s.set_grid(1.0 / N)
+            n, t = n_steps(dt, 0.4)
+            s.step(dt, n)
+            Q = s.prims()[:, 3:-3]
+            assert np.all(np.isfinite(Q))
+            ex = ER.solve(10.0, 13.33, 0.0, 1.0, 1e-6, 0.0, g, x, t)
+            errs[rs].append(float(np.mean(np.abs(Q[0] - ex[0]))))
+    for rs in errs:
+        e = errs[rs]
+        assert e[0] > e[1] > e[2], (rs, e)
+    assert all(c <= 1.05 * h for c, h in zip(errs[oracle.HLLC], errs[oracle.HLL])), errs
+    assert errs[oracle.HLLC][2] < 0.05, errs

@@ -71,3 +71,42 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     assert rc == _lib.ERR_ARG
     msg = _lib.lib().vb_noalloc_last_error().decode()
     assert "exceed the maximum" in msg
+
+
+def _device_state(dims, n, seed, gamma=4.0 / 3.0):
+    """Random primitive state in the reference layout built on the device
+    (C-order shape (n2+6, n1+6, n0+6, nv) = Fortran (nv, n0+6, n1+6, n2+6))."""
+    import torch
+
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    shp = tuple(x + 6 for x in reversed(n)) + (2 + dims,)
+    P = torch.empty(shp, dtype=torch.float64, device="cuda")
+    P[..., 0] = 1.0 + 0.2 * torch.rand(shp[:-1], generator=gen, device="cuda", dtype=torch.float64)
+    P[..., 1] = 3e-3 / (gamma - 1) * (1.0 + torch.rand(shp[:-1], generator=gen, device="cuda", dtype=torch.float64))
+    P[..., 2:] = 8.0 * torch.rand(shp[:-1] + (dims,), generator=gen, device="cuda", dtype=torch.float64) - 4.0
+    return P
+
+
+@pytest.mark.parametrize("dims,n", [(3, (512, 512, 512)), (1, (1 << 28,))])
+def test_noalloc_at_full_size(dims, n):
+    """The 512^3 grid of the 3D jet (4096 partial maxima, so the final
+    reduction loops over the scratch 16 times) and the largest 1D grid the
+    scratch accepts (2^28 cells: all 8192 partials), against the allocating
+    entry point."""
+    import torch
+
+    from verona_b200 import Solver
+
+    g = 4.0 / 3.0
+    out = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    P_dev = _device_state(dims, n, seed=7 + dims)
+    assert _noalloc(dims, n, g, P_dev, out) == 0
+    torch.cuda.synchronize()
+    got = float(out.item())
+    s = Solver(dims, n, g, (0.1,) * dims)
+    s.load_prims(P_dev)
+    del P_dev
+    ref = s.max_signal_speed()
+    s.close()
+    assert got > 0.0
+    assert abs(got - ref) <= 1e-14 * ref, (got, ref)

@@ -1,7 +1,7 @@
 """Mirror of the reference's Verona1D module (src/1dim/) over the B200 library.
 
 ParVector1D keeps arr1/arr2/arr3 (rho, u, u^x) on N cells with no ghosts;
-HARM_HLL (src/1dim/algos.jl:169-426) runs the reference's 1D scheme -- its
+HARM_HLL (src/1dim/algos.jl:58-315) runs the reference's 1D scheme -- its
 frozen end cells and persistent face arrays included -- in one persistent
 CTA on the device and returns the list of snapshots taken every `drops`.
 """
@@ -33,7 +33,7 @@ class ParVector1D:
 def HARM_HLL(P: ParVector1D, N: int, dt: float, dx: float, T: float, eos, drops: float, rec: str, *kwargs):
     """Verona1D.HARM_HLL(P, N, dt, dx, T, eos, drops, rec, n_iter, tol)."""
     if rec not in _REC:
-        raise ValueError("reconstruction not supported!")  # src/1dim/algos.jl:226-227
+        raise ValueError("reconstruction not supported!")  # src/1dim/algos.jl:115-116
     n_iter = int(kwargs[0]) if len(kwargs) > 0 else 50
     tol = float(kwargs[1]) if len(kwargs) > 1 else 1e-10  # UtoP's default, src/1dim/structs.jl:78
     gamma = eos.gamma if hasattr(eos, "gamma") else float(eos)

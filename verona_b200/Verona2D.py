@@ -52,7 +52,7 @@ def VectorLike(X):
 
 
 def turnoff_boundary(dt, T_exp, box_X):
-    """Built-in equivalent of examples/Jet2D/HARM_jet_breakout.jl:278-293: x-lo
+    """Built-in equivalent of examples/Jet2D/HARM_jet_breakout.jl:84-99: x-lo
     ghosts fixed with the decay of P[4] (u^y, as that example does) for
     box_X/3 < t < box_X, zero-gradient on y-lo, y-hi and x-hi."""
     return [(L.FACE["xlo"], L.BC_FIXED, (3, box_X / 3, box_X, 1 - dt / T_exp))] + [

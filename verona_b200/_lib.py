@@ -44,7 +44,8 @@ class VBOptions(C.Structure):
 
 class VBTuning(C.Structure):
     _fields_ = [("split_con2prim", C.c_int32), ("force_box", C.c_int32), ("learned_fused", C.c_int32),
-                ("fp32_pairs", C.c_int32), ("tma_tiles", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("fp32_pairs", C.c_int32), ("tma_tiles", C.c_int32), ("fp64_contract", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class VBIcParams(C.Structure):

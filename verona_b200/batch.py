@@ -38,6 +38,8 @@ def _sig():
         "vb_batch_get_time": [vp, C.c_int, C.POINTER(C.c_double)],
         "vb_batch_get_counters": [vp, C.POINTER(C.c_uint64), vp],
         "vb_batch_reset_counters": [vp, vp],
+        "vb_batch_check": [vp, vp],
+        "vb_batch_set_wait_limit": [vp, C.c_uint32],
         "vb_batch_num_variants": [C.c_int],
         "vb_batch_variant_shape": [C.c_int, C.c_int, ip, ip, ip],
         "vb_batch_set_tuning": [vp, C.c_int, C.c_int],
@@ -147,6 +149,19 @@ class Batch:
 
     def reset_counters(self, stream=None):
         _chk(self.lib.vb_batch_reset_counters(self._h, _stream_ptr(stream)), self._h)
+
+    def check(self, stream=None) -> int:
+        """vb_batch_check: synchronises and returns its status code (0, or
+        VB_ERR_TIMEOUT when a bounded wait of the batch kernel gave up) with
+        the message in self.last_error."""
+        rc = self.lib.vb_batch_check(self._h, _stream_ptr(stream))
+        self.last_error = self.lib.vb_batch_last_error(self._h).decode() if rc else ""
+        return rc
+
+    def set_wait_limit(self, max_polls: int = 0):
+        """Bound of a tile's wait for the previous stage, in polls of about
+        128 ns (0: the default, 2^24)."""
+        _chk(self.lib.vb_batch_set_wait_limit(self._h, int(max_polls)), self._h)
 
     def checkpoint(self, stream=None):
         _chk(self.lib.vb_batch_checkpoint(self._h, _stream_ptr(stream)), self._h)

@@ -3,6 +3,9 @@
 Translation units and their floating-point contract:
   vb_stage_f64.cu, vb_ref1d.cu, vb_api.cu  -fmad=false  (FP64 path rounds as
                                             the reference: no FMA contraction)
+  vb_stage_f64c.cu                          -fmad=true   (the FP64 stage kernels with FMA
+                                            contraction, namespace vb_f64c; tuning
+                                            fp64_contract)
   vb_stage_f32.cu                           -fmad=true, approximate FP32 divide and
                                             square root, FTZ (FP32-bulk path; the
                                             FP64 con2prim in it stays IEEE)
@@ -25,10 +28,13 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libverona_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", INC,
-          "--expt-relaxed-constexpr"]
+# -Werror=shadow: a local that shadows another (a loop counter named like a
+# physical constant) is a build error
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Werror=shadow", "-I", CSRC,
+          "-I", INC, "--expt-relaxed-constexpr"]
 UNITS = {
     "vb_stage_f64.cu": ["-fmad=false"],
+    "vb_stage_f64c.cu": ["-fmad=true"],
     "vb_ref1d.cu": ["-fmad=false"],
     "vb_api.cu": ["-fmad=false"],
     "vb_stage_f32.cu": ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],

@@ -1,7 +1,7 @@
 // C ABI of libverona_b200.so (include/verona_b200.h): handle lifecycle, state
 // buffers and the time-loop body that replaces the inner loop of the
 // reference's HARM_HLL (src/3dim/algos.jl:274-329, src/2dim/algos.jl:256-310,
-// src/1dim/algos.jl:200-424).
+// src/1dim/algos.jl:89-313).
 //
 // Device state of a 2D/3D handle (interior N, padded N+6 per axis):
 //   P[2]   primitive ping-pong buffers, SoA (one contiguous array per
@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/verona_b200.h"
@@ -54,7 +55,7 @@ struct vb_solver {
     size_t bytes = 0;
     std::string err;
     // kernel variants
-    vb_tuning tun{-1, 0, -1, -1, -1, {0, 0, 0}};
+    vb_tuning tun{-1, 0, -1, -1, -1, 0, {0, 0}};
     // TMA tensor maps of P[0], P[1] (the TMA forms of the stage kernels: 3D FP32, 2D)
     alignas(64) unsigned char tmap[2][128] = {};
     bool tmap_ok[2] = {false, false};
@@ -568,6 +569,10 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
         p.want_div = h->tun.learned_fused != 0;
     }
     const bool tma = h->tun.tma_tiles != 0;
+    // the FMA-contracted FP64 kernels (vb_stage_f64c.cu) for the plain FP64 path
+    const bool contract = std::is_same<R, double>::value && h->tun.fp64_contract == 1;
+    if (contract && vb_f64c_stage_params_size() != sizeof(StageParams))
+        return fail(h, VB_ERR_STATE, "vb_step: FMA-contracted FP64 unit built from another StageParams");
     auto stage = [&](const R* Pin, R* Pout, const double* Us, double* Uo, double dts, double a, double b) -> int {
         for (int d = 0; d < 3; ++d) p.dtdx[d] = d < h->dims ? dts / h->dx[d] : 0.0;
         p.tmap_in = nullptr;
@@ -583,8 +588,29 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
             VB_CUDA(h, cudaEventRecord(e0, s));
         }
         int nk = 0;
-        VB_CUDA(h, launch_stage<R>(h->dims, h->opt.recon, h->opt.riemann, p, bufs, s, &nk));
-        if (h->prof) VB_CUDA(h, cudaEventRecord(em, s));
+        if (h->prof && stage_split_c2p<R>(h->dims, p)) {
+            // the same two kernels as launch_stage would launch, with the
+            // profiling event between them: the stencil alone, then k_c2p
+            StageParams q = p;
+            q.skip_c2p = 1;
+            q.want_div = 0;
+            if (contract)
+                VB_CUDA(h, vb_f64c_launch_stage(h->dims, h->opt.recon, h->opt.riemann, &q, &bufs, s, &nk));
+            else
+                VB_CUDA(h, launch_stage<R>(h->dims, h->opt.recon, h->opt.riemann, q, bufs, s, &nk));
+            VB_CUDA(h, cudaEventRecord(em, s));
+            if (contract)
+                VB_CUDA(h, vb_f64c_launch_c2p(&p, &bufs, s));
+            else
+                VB_CUDA(h, launch_c2p<R>(p, bufs, s));
+            nk = 2;
+        } else {
+            if (contract)
+                VB_CUDA(h, vb_f64c_launch_stage(h->dims, h->opt.recon, h->opt.riemann, &p, &bufs, s, &nk));
+            else
+                VB_CUDA(h, launch_stage<R>(h->dims, h->opt.recon, h->opt.riemann, p, bufs, s, &nk));
+            if (h->prof) VB_CUDA(h, cudaEventRecord(em, s));
+        }
         if (p.skip_c2p) {
             // learned guess: the network's W per cell, then the W Newton from it
             StageParams q = p;
@@ -747,10 +773,10 @@ int vb_set_tuning(vb_handle h, const vb_tuning* t) {
     if (!h || !t) return fail(h, VB_ERR_ARG, "vb_set_tuning: null argument");
     if (t->split_con2prim < -1 || t->split_con2prim > 1 || t->force_box < 0 || t->force_box > 1 ||
         t->learned_fused < -1 || t->learned_fused > 1 || t->fp32_pairs < -1 || t->fp32_pairs > 1 ||
-        t->tma_tiles < -1 || t->tma_tiles > 1)
+        t->tma_tiles < -1 || t->tma_tiles > 1 || t->fp64_contract < 0 || t->fp64_contract > 1)
         return fail(h, VB_ERR_ARG,
-                    "vb_set_tuning: split_con2prim in {-1,0,1}, force_box in {0,1}, learned_fused, fp32_pairs and "
-                    "tma_tiles in {-1,0,1}");
+                    "vb_set_tuning: split_con2prim in {-1,0,1}, force_box and fp64_contract in {0,1}, learned_fused, "
+                    "fp32_pairs and tma_tiles in {-1,0,1}");
     h->tun = *t;
     return VB_OK;
 }

@@ -53,6 +53,7 @@ struct vb_batch {
     unsigned long long* cnt = nullptr;
     int cur = 0;
     int variant = 0, ctas_per_sm = 0, last_grid = 0;
+    unsigned max_polls = 0;  // 0: BATCH_MAX_POLLS
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
     cudaStream_t cap = nullptr;
     size_t bytes = 0;
@@ -176,6 +177,7 @@ template <typename R> static BatchLaunch<R> launch_desc(vb_batch_handle b, int n
     a.tol = b->opt.tol;
     a.n_iter = b->opt.n_iter;
     a.stats = b->opt.stats;
+    a.max_polls = b->max_polls ? b->max_polls : BATCH_MAX_POLLS;
     return a;
 }
 
@@ -376,6 +378,29 @@ int vb_batch_step(vb_batch_handle b, int nsteps, void* stream) {
 int vb_batch_get_time(vb_batch_handle b, int i, double* t) {
     if (!b || !t || i < 0 || i >= (int)b->probs.size()) return bfail(b, VB_ERR_ARG, "vb_batch_get_time: argument");
     *t = b->t[i];
+    return VB_OK;
+}
+
+int vb_batch_set_wait_limit(vb_batch_handle b, uint32_t max_polls) {
+    if (!b) return bfail(nullptr, VB_ERR_ARG, "null batch");
+    if (max_polls == b->max_polls) return VB_OK;
+    b->max_polls = max_polls;
+    drop_graphs(b);  // the limit is a kernel argument baked into the cached graphs
+    return VB_OK;
+}
+
+int vb_batch_check(vb_batch_handle b, void* stream) {
+    if (!b) return bfail(nullptr, VB_ERR_ARG, "null batch");
+    unsigned long long h[CNT_N];
+    BCUDA(b, cudaMemcpyAsync(h, b->cnt, sizeof h, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    BCUDA(b, cudaStreamSynchronize((cudaStream_t)stream));
+    if (h[CNT_TIMEOUT])
+        return bfail(b, VB_ERR_TIMEOUT,
+                     "vb_batch_check: %llu bounded waits of the batch kernel gave up; the state of the batch is "
+                     "undefined (vb_batch_rollback or reload it)",
+                     h[CNT_TIMEOUT]);
+    if (h[CNT_BAD_INDEX])
+        return bfail(b, VB_ERR_STATE, "vb_batch_check: %llu work items out of range were skipped", h[CNT_BAD_INDEX]);
     return VB_OK;
 }
 

@@ -14,8 +14,10 @@
 //     g - 1 of p are done: a per-problem completion counter, read with
 //     acquire semantics in a bounded wait. Every ticket a tile waits for is
 //     smaller than its own and is held by a CTA that is running, so the wait
-//     always ends; a wait that runs out (a fault elsewhere) counts
-//     CNT_TIMEOUT and stops the CTA.
+//     always ends; a wait that runs out (a fault elsewhere, or a limit set
+//     too small by vb_batch_set_wait_limit) counts CNT_TIMEOUT and stops the
+//     CTA. The tiles that depend on the stopped one then run out in turn, so
+//     the launch ends in bounded time; vb_batch_check reports it.
 //   * The tile itself is the box-tile stage body (stage_tile, vb_stage.cuh)
 //     with loads through L2, so data written earlier in the launch by other
 //     SMs is seen.
@@ -25,13 +27,14 @@
 //     examples' zero-gradient TurnOff) and writes the floored copy to the
 //     stage output; later stages copy the floored ghosts of their input.
 #pragma once
+#include "vb_ns.h"
 #include <type_traits>
 #include "vb_batch.h"
 #include "vb_stage.cuh"
 
-namespace vb {
+namespace VB_NS {
 
-constexpr unsigned BATCH_MAX_POLLS = 1u << 24;  // x ~128 ns: a few seconds
+constexpr unsigned BATCH_MAX_POLLS = 1u << 24;  // default wait bound, x ~128 ns: a few seconds
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
     unsigned long long v;
@@ -96,7 +99,7 @@ __global__ void __launch_bounds__(BATCH_NT) k_batch(BatchLaunch<R> a) {
             const unsigned long long need = (unsigned long long)g * (unsigned long long)pr.ntiles;
             int ok = 1;
             for (unsigned it = 0; ld_acquire_u64(a.done + e.p) < need; ++it) {
-                if (it >= BATCH_MAX_POLLS) {
+                if (it >= a.max_polls) {
                     ok = 0;
                     atomicAdd(a.counters + CNT_TIMEOUT, 1ULL);
                     break;

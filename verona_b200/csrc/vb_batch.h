@@ -1,11 +1,12 @@
 // Batched problems: the launch description shared by the batch kernel
 // (vb_batch.cuh) and its host API (vb_batch.cu).
 #pragma once
+#include "vb_ns.h"
 #include <cuda_runtime.h>
 
 #include "vb_internal.h"
 
-namespace vb {
+namespace VB_NS {
 
 constexpr int BATCH_NT = 256;  // threads per CTA of the batch kernel
 
@@ -29,7 +30,7 @@ template <typename R> struct BatchLaunch {
     long long T;             // tiles per stage
     long long total;         // nsteps * nstages * T
     int nstages, rk, cur0;   // cur0: P buffer holding the state at the first step
-    int riemann_unused;
+    unsigned max_polls;      // bound of a tile's wait for the previous stage (vb_batch_set_wait_limit)
     R* P0;
     R* P1;
     double* U0;

@@ -6,9 +6,10 @@
 // by the learned-guess path. Every loop is bounded by n_iter (or a fixed cap);
 // nothing here spins, traps or asserts -- failures are returned as codes.
 #pragma once
+#include "vb_ns.h"
 #include "vb_physics.cuh"
 
-namespace vb {
+namespace VB_NS {
 
 VB_HD double vb_nan() { return NAN; }
 
@@ -541,7 +542,7 @@ VB_HD int c2p_w(double g, const double* Uc, double W0, double rtol, int max_newt
     double lo = Wlo0, hi = fmax(2.0 * Wlo0, D - Q_t + 1.0);
     WRes rl = w_residual(k, D, Q_t, S2, lo);
     WRes rh = w_residual(k, D, Q_t, S2, hi);
-    for (int k = 0; k < 200 && rh.f * rl.f > 0.0; ++k) {
+    for (int grow = 0; grow < 200 && rh.f * rl.f > 0.0; ++grow) {
         hi *= 4.0;
         rh = w_residual(k, D, Q_t, S2, hi);
     }
@@ -550,7 +551,7 @@ VB_HD int c2p_w(double g, const double* Uc, double W0, double rtol, int max_newt
         return -(it + 1);
     }
     W = (W > lo && W < hi) ? W : 0.5 * (lo + hi);
-    for (int k = 0; k < max_bracket; ++k, ++it) {
+    for (int b = 0; b < max_bracket; ++b, ++it) {
         WRes r = w_residual(k, D, Q_t, S2, W);
         if ((r.f < 0.0) == (rl.f < 0.0)) {
             lo = W;

@@ -8,9 +8,10 @@
 // GPU and dominated the instruction count of these kernels. Callers keep the
 // interior cell count below 2^32.
 #pragma once
+#include "vb_ns.h"
 #include <stdint.h>
 
-namespace vb {
+namespace VB_NS {
 
 __host__ __device__ __forceinline__ uint32_t umulhi32(uint32_t a, uint32_t b) {
 #ifdef __CUDA_ARCH__

@@ -1,9 +1,10 @@
 // Internal interfaces between the kernel translation units and the C ABI.
 #pragma once
+#include "vb_ns.h"
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-namespace vb {
+namespace VB_NS {
 
 constexpr int NG = 3;  // ghost cells per side, as the reference's ParVector2D/3D
 
@@ -101,7 +102,7 @@ template <typename R>
 cudaError_t launch_max_speed(const Grid& g, const R* P, double gamma, double* partial, int max_partial,
                              double* out, cudaStream_t s);
 
-// 1D reference solver (src/1dim/algos.jl:169-426), FP64, one persistent CTA.
+// 1D reference solver (src/1dim/algos.jl:58-315), FP64, one persistent CTA.
 struct Ref1DState {
     int N;
     double *P, *Ph, *U, *Uh, *PL, *PR, *F;  // [3][N] each
@@ -125,6 +126,11 @@ template <typename R> bool encode_stage_tmap(void* out, const R* P, const Grid& 
 // 1 when launch_stage with these arguments leaves the FP32 divergence in Pout
 // for the caller's con2prim kernel (z-pair kernel with skip_c2p and want_div)
 template <typename R> int stage_div_in_pout(int dims, int rec, int rs, const StageParams& p);
+// 1 when launch_stage with these arguments launches the stencil kernel and then
+// the split con2prim kernel k_c2p (3D z-marching stage, split con2prim); the
+// same work is then launch_stage with skip_c2p = 1 and want_div = 0 followed
+// by launch_c2p (the profiling path records an event between the two)
+template <typename R> int stage_split_c2p(int dims, const StageParams& p);
 
 // split con2prim of a 3D stage on its own (vb_stage_zm.cuh)
 template <typename R> cudaError_t launch_c2p(const StageParams& p, const StageBufs<R>& b, cudaStream_t s);
@@ -149,3 +155,12 @@ cudaError_t launch_point_c2p_w(double g, const double* U, const double* W0, doub
                                int max_bracket, double* P, int* iters, int* fallback, int n, cudaStream_t s);
 
 }  // namespace vb
+
+// FP64 stage kernels built with FMA contraction (vb_stage_f64c.cu, namespace
+// vb_f64c): launch_stage<double> and launch_c2p<double> of that unit. p and b
+// point to the caller's StageParams and StageBufs<double> (the same header, so
+// the same layout; vb_f64c_stage_params_size() lets the caller check it).
+cudaError_t vb_f64c_launch_stage(int dims, int rec, int rs, const void* p, const void* b, cudaStream_t s,
+                                 int* kernels);
+cudaError_t vb_f64c_launch_c2p(const void* p, const void* b, cudaStream_t s);
+size_t vb_f64c_stage_params_size();

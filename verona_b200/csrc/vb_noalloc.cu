@@ -13,13 +13,19 @@
 // The scratch is a file-scope `static __device__` array: every GPU that
 // loads the library holds its 64 KiB until the process exits. Host code must
 // not pass the array's name to a kernel (on the host it is only a stand-in,
-// not a device address); its device address is looked up once per device
-// with cudaGetSymbolAddress, on the first call made while that device is
-// current, and cached. Make that first call on a device before any stream
-// capture. All calls share the one array and it keeps the last call's
-// contents: each call writes every partial it later reads, so nothing needs
-// clearing, but two calls whose kernels overlap on the GPU (different
-// streams, no ordering between them) race on it.
+// not a device address); its device address is looked up with
+// cudaGetSymbolAddress on the first call made while a device is current, and
+// cached together with that device's SM count and the CUDA context it was
+// looked up in. A call made in another context of the same device (after
+// cudaDeviceReset, or after the host reset the device) looks both up again,
+// so an address of a destroyed context is never used. Make the first call on
+// a device, and the first after a reset, before any stream capture. All calls
+// share the one array and it keeps the last call's contents: each call writes
+// every partial it later reads, so nothing needs clearing, but two calls
+// whose kernels overlap on the GPU (different streams, no ordering between
+// them) race on it.
+#include <cuda.h>
+#include <cudaTypedefs.h>  // PFN_cuCtxGetCurrent
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -74,23 +80,57 @@ __global__ void __launch_bounds__(NA_THREADS) k_max_reduce_to(const double* __re
     if (threadIdx.x == 0) *out = m;
 }
 
-// device address of vb_noalloc_partial, looked up once per device
-static double* g_partial_addr[NA_MAX_DEVICES] = {};
-static std::mutex g_partial_mu;
+// device address of vb_noalloc_partial and the SM count, looked up once per
+// device and context
+struct NaDevice {
+    CUcontext ctx;
+    double* partial;
+    int sms;
+};
+static NaDevice g_na_dev[NA_MAX_DEVICES] = {};
+static std::mutex g_na_mu;
 
-static cudaError_t scratch_for_current_device(double** out) {
+// cuCtxGetCurrent through the runtime's entry-point query (no driver library
+// is linked); nullptr where the driver does not provide it
+static PFN_cuCtxGetCurrent_v4000 ctx_getter() {
+    static PFN_cuCtxGetCurrent_v4000 fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f);
+    }();
+    return fn;
+}
+
+static cudaError_t scratch_for_current_device(double** out, int* sms) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= NA_MAX_DEVICES) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_partial_mu);
-    if (!g_partial_addr[dev]) {
+    PFN_cuCtxGetCurrent_v4000 get = ctx_getter();
+    if (!get) return cudaErrorNotSupported;
+    // the context current on this thread; null before the runtime has made the
+    // device's primary context current (cudaGetSymbolAddress does that)
+    CUcontext ctx = nullptr;
+    if (get(&ctx) != CUDA_SUCCESS) return cudaErrorNotSupported;
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    NaDevice& d = g_na_dev[dev];
+    if (!d.partial || !ctx || d.ctx != ctx) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, vb_noalloc_partial);
         if (e != cudaSuccess) return e;
-        g_partial_addr[dev] = static_cast<double*>(p);
+        int n = 0;
+        e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        if (get(&ctx) != CUDA_SUCCESS || !ctx) return cudaErrorNotSupported;
+        d.ctx = ctx;
+        d.partial = static_cast<double*>(p);
+        d.sms = n > 0 ? n : 1;
     }
-    *out = g_partial_addr[dev];
+    *out = d.partial;
+    *sms = d.sms;
     return cudaSuccess;
 }
 
@@ -112,6 +152,7 @@ static int na_fail(int code, const char* msg, cudaError_t e = cudaSuccess) {
 
 extern "C" int vb_max_signal_speed_noalloc(int dims, int nx, int ny, int nz, double gamma, const double* P_aos_dev,
                                            double* c_dev, void* stream) {
+    g_na_err[0] = 0;
     if (dims < 1 || dims > 3) return na_fail(VB_ERR_ARG, "dims must be 1, 2 or 3");
     if (!P_aos_dev || !c_dev) return na_fail(VB_ERR_ARG, "null array");
     int nn[3] = {nx, dims > 1 ? ny : 1, dims > 2 ? nz : 1};
@@ -126,15 +167,16 @@ extern "C" int vb_max_signal_speed_noalloc(int dims, int nx, int ny, int nz, dou
         return VB_ERR_ARG;
     }
     double* partial = nullptr;
-    cudaError_t e = scratch_for_current_device(&partial);
+    int sms = 1;
+    cudaError_t e = scratch_for_current_device(&partial, &sms);
     if (e != cudaSuccess) return na_fail(VB_ERR_CUDA, "cudaGetSymbolAddress", e);
     // enough blocks that no thread covers more than NA_CELLS_PER_THREAD cells,
     // and at least enough to fill the GPU (4 per SM) unless the grid is tiny;
     // at most NA_MAX_BLOCKS because cells <= NA_MAX_CELLS
     const long long per_block = (long long)NA_THREADS * NA_CELLS_PER_THREAD;
     const long long need = (cells + per_block - 1) / per_block;
-    const long long fill = std::min((cells + NA_THREADS - 1) / NA_THREADS, 148LL * 4);
-    const int nb = (int)std::max(need, fill);
+    const long long fill = std::min((cells + NA_THREADS - 1) / NA_THREADS, 4LL * sms);
+    const int nb = (int)std::min<long long>(std::max(need, fill), NA_MAX_BLOCKS);
     cudaStream_t s = (cudaStream_t)stream;
     const int n0 = nn[0] + 2 * NG, n1 = dims > 1 ? nn[1] + 2 * NG : 1, n2 = dims > 2 ? nn[2] + 2 * NG : 1;
     if (dims == 1) k_max_speed_aos<1><<<nb, NA_THREADS, 0, s>>>(n0, n1, n2, P_aos_dev, gamma, partial);

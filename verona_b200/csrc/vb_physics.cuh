@@ -8,13 +8,14 @@
 // to the reference's rounding (IEEE +,-,*,/,sqrt are correctly rounded on
 // sm_100a). The FP32 unit uses the same code with FP32 constants.
 #pragma once
+#include "vb_ns.h"
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 
 #define VB_HD __host__ __device__ __forceinline__
 
-namespace vb {
+namespace VB_NS {
 
 enum { REC_MINMOD = 0, REC_PPM = 1, REC_WENOZ = 2 };
 enum { RS_HLL = 0, RS_HLLC = 1 };

@@ -1,11 +1,11 @@
-// The reference's 1D solver, Verona1D.HARM_HLL (src/1dim/algos.jl:169-426),
+// The reference's 1D solver, Verona1D.HARM_HLL (src/1dim/algos.jl:58-315),
 // FP64, as one persistent CTA that runs every step of a call: each phase of
 // the Julia loop becomes a block-wide pass over the N cells separated by
 // __syncthreads(), so a whole shock-tube run is a single launch.
 //
 // The reference keeps state between stages that this kernel keeps too: the
 // face arrays PL/PR start as copies of P and are only refreshed on the ranges
-// the Julia loops write (src/1dim/algos.jl:202-228), so the edge faces keep
+// the Julia loops write (src/1dim/algos.jl:91-117), so the edge faces keep
 // their t = 0 values; cells 1, N-1, N (1-based) of U are never updated.
 // Compiled with -fmad=false: bit-identical to the oracle restatement.
 #include "vb_con2prim.cuh"
@@ -36,7 +36,7 @@ __device__ void ref1d_stage(const Ref1DState& st, const double* P, const double*
                             double g, int rec) {
     const int N = st.N;
     const int tid = threadIdx.x;
-    // src/1dim/algos.jl:202-228
+    // src/1dim/algos.jl:91-117
     if (rec == REC_MINMOD) {
         for (int i = 1 + tid; i <= N - 2; i += blockDim.x)
             for (int v = 0; v < 3; ++v) {

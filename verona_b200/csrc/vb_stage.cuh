@@ -14,6 +14,7 @@
 // the guess and writes U and the floored P. In 2D the tile with its halo
 // along both axes can instead come as one TMA tile (TMA form of k_stage).
 #pragma once
+#include "vb_ns.h"
 #include <cuda.h>  // CUtensorMap
 
 #include "vb_con2prim.cuh"
@@ -22,7 +23,7 @@
 #include "vb_tc.cuh"
 #include "vb_tmap.h"
 
-namespace vb {
+namespace VB_NS {
 
 template <int DIM> struct TileCfg;
 template <> struct TileCfg<3> { static constexpr int TX = 32, TY = 4, TZ = 4, NT = 256; };
@@ -231,7 +232,14 @@ __device__ __forceinline__ void stage_tile(const StageParams& p, const StageBufs
         }
         const bool ok = tc::mbar_wait(sBar, 0, nullptr, TILE_MAX_POLLS);
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) count_add(p.counters, CNT_TIMEOUT, 1);
+            // the box may still be landing in this CTA's shared memory: thread 0
+            // waits once more (bounded) before the CTA ends, so that the CTA
+            // stays resident while the copy completes; if that wait runs out
+            // too, the copy is still outstanding when the CTA exits
+            if (tid == 0) {
+                count_add(p.counters, CNT_TIMEOUT, 1);
+                tc::mbar_wait(sBar, 0, nullptr, TILE_MAX_POLLS);
+            }
             return;
         }
     }
@@ -867,6 +875,7 @@ cudaError_t launch_max_speed(const Grid& g, const R* P, double gamma, double* pa
     template cudaError_t launch_bc_decay<R>(const Grid&, R*, int, int, double, cudaStream_t);        \
     template cudaError_t launch_max_speed<R>(const Grid&, const R*, double, double*, int, double*,   \
                                              cudaStream_t);                                          \
-    template int stage_div_in_pout<R>(int, int, int, const StageParams&);
+    template int stage_div_in_pout<R>(int, int, int, const StageParams&);                             \
+    template int stage_split_c2p<R>(int, const StageParams&);
 
 }  // namespace vb

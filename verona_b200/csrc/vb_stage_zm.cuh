@@ -19,11 +19,12 @@
 // (x, y, z), then the RK combination, con2prim (guess = this stage's P) and
 // the floors, as in k_stage.
 #pragma once
+#include "vb_ns.h"
 #include <type_traits>
 
 #include "vb_stage.cuh"
 
-namespace vb {
+namespace VB_NS {
 
 template <int TX, int TY> struct ZmGeom {
     static constexpr int NV = 5, NT = TX * TY;
@@ -427,6 +428,14 @@ cudaError_t launch_stage_zm(const StageParams& p, const StageBufs<R>& b, cudaStr
 template <typename R> int stage_div_in_pout(int dims, int rec, int rs, const StageParams& p) {
     if (!std::is_same<R, float>::value || dims != 3 || p.force_box || !zm_fits<R>(p)) return 0;
     return p.pairs && zp_available(rec, rs) && p.skip_c2p && p.want_div ? 1 : 0;
+}
+
+// 1 when launch_stage with these arguments runs the stencil kernel and then
+// k_c2p as a kernel of its own (a split 3D z-marching stage); the same two
+// launches result from launch_stage with skip_c2p = 1, want_div = 0 followed
+// by launch_c2p
+template <typename R> int stage_split_c2p(int dims, const StageParams& p) {
+    return dims == 3 && !p.force_box && zm_fits<R>(p) && p.split && !p.skip_c2p ? 1 : 0;
 }
 
 template <typename R>

@@ -23,12 +23,13 @@
 // FP64 exactly as in k_stage_zm. Same scheme as the reference's 3D kernels
 // (src/3dim/algos.jl:14-200, src/fluxlimiter.jl:19-71) plus HLLC.
 #pragma once
+#include "vb_ns.h"
 #include <cuda.h>  // CUtensorMap
 
 #include "vb_stage_zm.cuh"
 #include "vb_tc.cuh"
 
-namespace vb {
+namespace VB_NS {
 namespace pk {
 
 using f2 = float2;

@@ -13,10 +13,11 @@
 // Every wait on an mbarrier is bounded; a wait that runs out sets *err and
 // returns false, so callers can skip the remaining work, free TMEM and exit.
 #pragma once
+#include "vb_ns.h"
 #include <cuda_bf16.h>
 #include <stdint.h>
 
-namespace vb {
+namespace VB_NS {
 namespace tc {
 
 // byte offset of element (row, k) in a K-major no-swizzle operand of R rows

@@ -2,12 +2,13 @@
 // (cuTensorMapEncodeTiled) is reached through the runtime's entry-point query,
 // so the library links no driver library.
 #pragma once
+#include "vb_ns.h"
 #include <cuda.h>
 #include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-namespace vb {
+namespace VB_NS {
 
 inline PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {

@@ -176,15 +176,15 @@ class Solver:
         L.check(L.lib().vb_reset_counters(self._h, _stream_ptr(stream)), self._h)
 
     def set_tuning(self, split_con2prim: int = -1, force_box: int = 0, learned_fused: int = -1, fp32_pairs: int = -1,
-                   tma_tiles: int = -1):
-        t = L.VBTuning(split_con2prim, force_box, learned_fused, fp32_pairs, tma_tiles)
+                   tma_tiles: int = -1, fp64_contract: int = 0):
+        t = L.VBTuning(split_con2prim, force_box, learned_fused, fp32_pairs, tma_tiles, fp64_contract)
         L.check(L.lib().vb_set_tuning(self._h, C.byref(t)), self._h)
 
     def get_tuning(self) -> dict:
         t = L.VBTuning()
         L.check(L.lib().vb_get_tuning(self._h, C.byref(t)), self._h)
         return {"split_con2prim": t.split_con2prim, "force_box": t.force_box, "learned_fused": t.learned_fused,
-                "fp32_pairs": t.fp32_pairs, "tma_tiles": t.tma_tiles}
+                "fp32_pairs": t.fp32_pairs, "tma_tiles": t.tma_tiles, "fp64_contract": t.fp64_contract}
 
     def profile(self, enable: bool = True):
         L.check(L.lib().vb_profile_enable(self._h, int(enable)), self._h)
