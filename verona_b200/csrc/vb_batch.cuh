@@ -34,8 +34,6 @@
 
 namespace VB_NS {
 
-constexpr unsigned BATCH_MAX_POLLS = 1u << 24;  // default wait bound, x ~128 ns: a few seconds
-
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
     unsigned long long v;
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");

@@ -9,6 +9,7 @@
 namespace VB_NS {
 
 constexpr int BATCH_NT = 256;  // threads per CTA of the batch kernel
+constexpr unsigned BATCH_MAX_POLLS = 1u << 24;  // default wait bound, x ~128 ns: a few seconds
 
 struct BatchProb {
     int dims, rec;
