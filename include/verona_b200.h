@@ -58,9 +58,12 @@ enum { VB_RK2 = 2, VB_RK3 = 3 };
 /* precision: FP64 everywhere (reference), or FP32 reconstruction/flux/divergence with
  * FP64 conserved variables, RK accumulation and con2prim */
 enum { VB_PREC_FP64 = 0, VB_PREC_FP32_BULK = 1 };
-/* con2prim initial guess: the cell's previous primitive state (reference) or the
- * learned BF16 MLP guess refined by Newton (3D only) */
-enum { VB_GUESS_PREVIOUS = 0, VB_GUESS_LEARNED = 1 };
+/* con2prim initial guess: the cell's previous primitive state with the
+ * reference's con2prim cascade (reference); the learned BF16 MLP guess
+ * refined by the W Newton (3D only); or the previous state's W refined by that
+ * same W Newton (3D only: the learned path without the network, the baseline
+ * of what the network gains) */
+enum { VB_GUESS_PREVIOUS = 0, VB_GUESS_LEARNED = 1, VB_GUESS_PREVIOUS_W = 2 };
 /* boundary kinds of vb_set_boundary */
 enum {
     VB_BC_OUTFLOW = 0, /* zero-gradient copy of the first interior cell (TurnOff's y/z/x-high copies) */
@@ -76,6 +79,7 @@ enum {
     VB_CNT_C2P_CELLS = 3,    /* cells solved (options.stats = 1) */
     VB_CNT_TIMEOUT = 4,      /* bounded device waits that gave up */
     VB_CNT_BAD_INDEX = 5,    /* out-of-range work items that were skipped */
+    VB_CNT_C2P_FP64 = 6,     /* cells solved by the FP64 Newton (options.stats = 1; learned guess) */
     VB_CNT_N = 8
 };
 
@@ -92,14 +96,19 @@ typedef struct vb_options {
     double floor_;        /* density / internal-energy floor: HARM_HLL `floor` */
     double w_rtol;        /* learned guess: relative W tolerance of the refinement (1e-12) */
     int32_t w_max_newton; /* learned guess: Newton steps before the bracketed fallback (8) */
-    int32_t reserved_i[7];
+    int32_t c2p_fp32;     /* W-Newton guesses + FP32 bulk: 1 = precision-gated con2prim (default): an
+                           * FP32 Newton on the pressure where the guess has Lorentz factor below
+                           * sqrt 2 and kinetic energy below 10 x the pressure, the FP64 W Newton
+                           * elsewhere; 0 = the FP64 W Newton on every cell */
+    int32_t reserved_i[6];
     double reserved_d[4];
 } vb_options;
 
 typedef struct vb_solver* vb_handle;
 
 /* Fill *o with the reference's defaults (WENOZ, HLL, RK2, FP64, previous-state
- * guess, n_iter 50, tol 1e-10, floor 1e-7). */
+ * guess, n_iter 50, tol 1e-10, floor 1e-7) and the extensions' (w_rtol 1e-12,
+ * w_max_newton 8, c2p_fp32 1). */
 int vb_default_options(vb_options* o);
 
 /* Create a solver for an nx x ny x nz interior grid (ny = nz = 1 in 1D,
@@ -206,7 +215,7 @@ int vb_reset_counters(vb_handle h, void* stream);
  * the W Newton from it run in one kernel; 0 = a guess kernel writes one W per
  * cell and the con2prim kernel reads it; -1 = library default (1). Both start
  * the Newton from the same FP32-rounded guess.
- * fp32_pairs (precision = VB_PREC_FP32_BULK, 3D, WENOZ with HLL or HLLC): 1 =
+ * fp32_pairs (precision = VB_PREC_FP32_BULK, 3D, every reconstruction with HLL or HLLC): 1 =
  * the z-pair stencil kernel (two cells per thread on packed FP32 pairs);
  * 0 = one cell per thread; -1 = library default (1). The two agree to FP32
  * rounding, not bitwise.
@@ -321,8 +330,10 @@ int vb_attach_mlp(vb_handle h, vb_mlp_handle m);
  * held on every GPU that loads the library until the process exits. The
  * interior may have at most 8192 x 256 x 128 = 268,435,456 cells; larger
  * grids are rejected with VB_ERR_ARG. The first call on a device looks up the
- * scratch address on that device (make it before any stream capture). Calls
- * share the scratch, so two calls whose kernels overlap on the GPU race.
+ * scratch address and the SM count on that device, and again the first call
+ * in a new CUDA context of it (after cudaDeviceReset); make those calls before
+ * any stream capture. Calls share the scratch, so two calls whose kernels
+ * overlap on the GPU race.
  * Errors: vb_noalloc_last_error(). */
 int vb_max_signal_speed_noalloc(int dims, int nx, int ny, int nz, double gamma, const double* P_aos_dev,
                                 double* c_dev, void* stream);
@@ -335,6 +346,14 @@ const char* vb_noalloc_last_error(void);
  * where the bracketed phase ran. No counterpart in the reference. */
 int vb_point_c2p_w(double gamma, const double* U, const double* W0, double rtol, int max_newton, int max_bracket,
                    double* P, int* iters, int* fallback, int n, void* stream);
+/* The same refinement with the precision gate of the FP32-bulk learned path
+ * (options.c2p_fp32): from the FP32 guesses W0 (n), an FP32 Newton on the
+ * pressure where the guess has Lorentz factor below sqrt 2 and kinetic energy
+ * below 10 x the guessed pressure (converged to |dp| <= 4e-7 p), else the FP64
+ * W Newton of vb_point_c2p_w; fp64 (may be NULL) receives 1 where the FP64
+ * Newton ran. No counterpart in the reference. */
+int vb_point_c2p_gated(double gamma, const double* U, const float* W0, double rtol, int max_newton, int max_bracket,
+                       double* P, int* iters, int* fp64, int n, void* stream);
 
 /* ---- grid kernels one at a time (the reference's kernels as separate calls) ------
  * Caller-owned device arrays in the reference layout: FP64 AoS (2 + dims,
@@ -370,7 +389,8 @@ const char* vb_grid_last_error(void);
  * Many 1D and 2D problems of uneven size advance together. Each has its own
  * interior size, reconstruction, cell widths and time step; all share gamma
  * and the options' riemann, rk, precision (FP64 or FP32 bulk), n_iter, tol
- * and floor_ (guess must be VB_GUESS_PREVIOUS), and every face is outflow.
+ * and floor_ (guess must be VB_GUESS_PREVIOUS); every face is outflow unless
+ * vb_batch_set_boundary gives it another kind.
  * Each problem evolves exactly as a single-grid handle of the same dims and
  * options with 3 ghost cells would. vb_batch_step runs nsteps steps of every
  * problem as ONE persistent kernel launch, replayed from a CUDA graph: tiles
@@ -392,6 +412,14 @@ int vb_batch_create(vb_batch_handle* b, int nprob, const vb_batch_problem* probs
                     const vb_options* o);
 int vb_batch_destroy(vb_batch_handle b);
 const char* vb_batch_last_error(vb_batch_handle b); /* NULL handle: the last failed create */
+/* Boundary of face `face` (VB_FACE_XLO .. VB_FACE_YHI; x faces only in 1D) of
+ * problem i, with the kinds and parameters of vb_set_boundary: OUTFLOW (the
+ * default on every face), FIXED (the loaded ghosts, with an optional decay
+ * {var, t_on, t_off, factor} by the problem's own time) or NOZZLE {radius, c1,
+ * c2, rho, u, u1[, u2]} -- so jets run in a batch, as Verona2D.HARM_HLL with
+ * the examples' boundary callback (examples/Jet2D/HARM_jet_breakout.jl:84-99)
+ * would run them one at a time. Synchronises the device. */
+int vb_batch_set_boundary(vb_batch_handle b, int i, int face, int kind, const double* params, int nparams);
 /* problem i's primitives, FP64 AoS (2 + dims, nx + 6 [, ny + 6]) as vb_load_prims */
 int vb_batch_load_prims(vb_batch_handle b, int i, const double* P_aos, void* stream);
 int vb_batch_store_prims(vb_batch_handle b, int i, double* P_aos, void* stream);

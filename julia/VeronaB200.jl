@@ -52,7 +52,8 @@ struct VBOptions
     floor_::Float64
     w_rtol::Float64
     w_max_newton::Int32
-    reserved_i::NTuple{7,Int32}
+    c2p_fp32::Int32
+    reserved_i::NTuple{6,Int32}
     reserved_d::NTuple{4,Float64}
 end
 
@@ -106,7 +107,7 @@ function options(; recon = :wenoz, riemann = :hll, rk = 2, precision = :fp64, gu
     check(ccall((:vb_default_options, libvb), Cint, (Ref{VBOptions},), o), C_NULL)
     x = o[]
     return VBOptions(x.version, RECON[recon], RIEMANN[riemann], rk, PRECISION[precision], GUESS[guess], n_iter, 0,
-                     tol, floor, x.w_rtol, x.w_max_newton, x.reserved_i, x.reserved_d)
+                     tol, floor, x.w_rtol, x.w_max_newton, x.c2p_fp32, x.reserved_i, x.reserved_d)
 end
 
 # ---- a solver handle ------------------------------------------------------------

@@ -68,6 +68,60 @@ int main() {
         std::printf("the bracketed phase never ran\n");
         return 1;
     }
+    // the precision-gated refinement of the FP32-bulk learned path
+    // (c2p_w_gated): states with Lorentz factor up to 3 and p / rho down to
+    // 1e-6, guesses 0.1 % off in W (for cold gas that puts the guessed
+    // pressure far above the true one), rounded to FP32. Cells the gate admits are solved in FP32 and must
+    // match the exact state to FP32 accuracy (rho and the four-velocity to
+    // 1e-6 relative, the internal energy to 2e-5); the rest go to the FP64 W
+    // Newton and must reproduce U to 1e-9.
+    int n32 = 0, n64 = 0;
+    for (int i = 0; i < n && bad < 5; ++i) {
+        const double g = (i & 1) ? 4.0 / 3.0 : 5.0 / 3.0;
+        const double rho = std::pow(10.0, -4.0 + 5.0 * urand());
+        const double p = rho * std::pow(10.0, -6.0 + 8.0 * urand());
+        const double lor = std::pow(10.0, std::log10(3.0) * urand());
+        double d[3] = {urand() - 0.5, urand() - 0.5, urand() - 0.5};
+        const double nd = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) + 1e-300;
+        const double um = std::sqrt(lor * lor - 1.0);
+        double P[5] = {rho, p / (g - 1.0), um * d[0] / nd, um * d[1] / nd, um * d[2] / nd};
+        double U[5];
+        prim2con<3>(g, P, U);
+        const double W = (P[0] + g * P[1]) * lor * lor;
+        const float W0 = (float)(W * (1.0 + 1e-3 * (2.0 * urand() - 1.0)));
+        double R[5];
+        int fb = 0, f64 = -1;
+        const int it = c2p_w_gated(g, U, W0, 1e-12, 8, 400, true, R, &fb, &f64);
+        const bool floored = rho / lor < 2e-8 || p / (g - 1.0) < 2e-8;
+        bool good = it > 0;
+        if (good && !f64) {
+            ++n32;
+            const double er = std::fabs(R[0] - P[0]) / P[0];
+            const double eu = std::fabs(R[1] - P[1]) / P[1];
+            double ev = 0.0;
+            for (int v = 2; v < 5; ++v) ev = std::fmax(ev, std::fabs(R[v] - P[v]));
+            good = floored || (er <= 1e-6 && eu <= 2e-5 && ev <= 1e-6 * lor);
+        } else if (good) {
+            ++n64;
+            double V[5], scale = 0.0, err = 0.0;
+            prim2con<3>(g, R, V);
+            for (int v = 0; v < 5; ++v) {
+                scale = std::fmax(scale, std::fabs(U[v]));
+                err = std::fmax(err, std::fabs(V[v] - U[v]));
+            }
+            good = floored || err <= 1e-9 * scale;
+        }
+        if (!good) {
+            std::printf("gated state %d: it %d fp64 %d rho %.3e p %.3e lorentz %.3f -> %.9e %.9e\n", i, it, f64, rho, p,
+                        lor, R[0], R[1] * (g - 1.0));
+            ++bad;
+        }
+    }
+    if (bad) return 1;
+    if (n32 < n / 10 || n64 < n / 10) {
+        std::printf("gate split %d FP32 / %d FP64: both paths must run\n", n32, n64);
+        return 1;
+    }
     std::printf("ok\n");
     return 0;
 }

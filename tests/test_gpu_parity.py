@@ -286,13 +286,16 @@ def test_zmarch_kernel_parity(oracle, rec, rs, rk, variant):
 
 @pytest.mark.parametrize("rs", ["hll", "hllc"])
 @pytest.mark.parametrize("variant", ["split", "fused"])
-def test_fp32_pair_kernel_matches_scalar_kernel(rs, variant):
+@pytest.mark.parametrize("rec", ["wenoz", "ppm", "minmod"])
+def test_fp32_pair_kernel_matches_scalar_kernel(rs, variant, rec):
     """The z-pair FP32 stencil kernel (two cells per thread on packed FP32
     instructions) against the one-cell-per-thread FP32 kernel and the FP64
-    path. 69 cells in z give a 64-cell range and a 5-cell range, whose last
-    pair is incomplete. The two FP32 kernels round differently (hand-written
-    packed contraction, folded constants), so they agree to FP32 rounding, and
-    each stays within the FP32-bulk error bar of the FP64 run."""
+    path, for every reconstruction (WENOZ on packed pairs; PPM and MINMOD
+    lane by lane through the scalar FP32 limiters). 69 cells in z give a
+    64-cell range and a 5-cell range, whose last pair is incomplete. The two
+    FP32 kernels round differently (hand-written packed contraction, folded
+    constants, the HLL / HLLC flux), so they agree to FP32 rounding, and each
+    stays within the FP32-bulk error bar of the FP64 run."""
     from verona_b200 import Solver
 
     g = 4.0 / 3.0
@@ -302,7 +305,7 @@ def test_fp32_pair_kernel_matches_scalar_kernel(rs, variant):
     dt = 0.4 / sum(1.0 / d for d in dxs)
     out = {}
     for name, prec, pairs in (("fp64", "fp64", 0), ("scalar", "fp32", 0), ("pairs", "fp32", 1)):
-        s = Solver(3, n, g, dxs, recon="wenoz", riemann=rs, rk=3, precision=prec, n_iter=50, tol=1e-12, floor=1e-8)
+        s = Solver(3, n, g, dxs, recon=rec, riemann=rs, rk=3, precision=prec, n_iter=50, tol=1e-12, floor=1e-8)
         s.set_tuning(split_con2prim=int(variant == "split"), fp32_pairs=pairs)
         s.set_boundary(0, 2, nozzle_params(3, n, 5.0, gamma=g))
         s.load_prims(P0)
@@ -317,11 +320,11 @@ def test_fp32_pair_kernel_matches_scalar_kernel(rs, variant):
     for v in range(5):
         d = l1(out["pairs"], out["scalar"], v) if v < 2 else float(
             np.mean(np.abs(out["pairs"][v] - out["scalar"][v])))
-        print(rs, variant, "var", v, "pairs vs scalar FP32:", d)
+        print(rec, rs, variant, "var", v, "pairs vs scalar FP32:", d)
         assert d < 2e-6
     for name in ("scalar", "pairs"):
         e = (l1(out[name], out["fp64"], 0), l1(out[name], out["fp64"], 1))
-        print(rs, variant, name, "L1 rho, p vs FP64:", e)
+        print(rec, rs, variant, name, "L1 rho, p vs FP64:", e)
         assert max(e) < 1e-5
 
 
@@ -514,6 +517,8 @@ def test_fp64_1d_2d_inflow_within_parity_bar(oracle, dims, contract):
     P0 = jet_ic(dims, n, gamma=g, noise=0.03, seed=24)
     dxs = [1.0 / n[0]] * dims
     dt = 0.4 / sum(1.0 / d for d in dxs)
+    if dims == 1:
+        P0[2, :3] = 3.0  # an inflow into the tube through the x-lo ghosts
     s = Solver(dims, n[:dims], g, dxs, recon="wenoz", riemann="hllc", rk=3, n_iter=50, tol=1e-12, floor=1e-8)
     s.set_tuning(fp64_contract=contract)
     o = oracle.SolverND(dims, n[:dims], P0, g, 1e-8, 50, 1e-12, oracle.WENOZ, oracle.HLLC, 3)
@@ -523,7 +528,6 @@ def test_fp64_1d_2d_inflow_within_parity_bar(oracle, dims, contract):
         s.set_boundary(0, 2, noz)
         o.set_boundary(0, oracle.BC_NOZZLE, noz)
     else:
-        P0[2, :3] = 3.0  # an inflow into the tube through the x-lo ghosts
         s.set_boundary(0, 1)
         o.set_boundary(0, oracle.BC_FIXED, (-1.0, 0.0, 0.0, 1.0))
     s.load_prims(P0)

@@ -16,10 +16,10 @@ OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_UNSUPPORTED, ERR_NOMEM, ERR_TIMEOUT = 0, -
 RECON = {"minmod": 0, "ppm": 1, "wenoz": 2, "MINMOD": 0, "PPM": 1, "WENOZ": 2}
 RIEMANN = {"hll": 0, "hllc": 1, "HLL": 0, "HLLC": 1}
 PRECISION = {"fp64": 0, "fp32": 1, "fp32_bulk": 1}
-GUESS = {"previous": 0, "learned": 1}
+GUESS = {"previous": 0, "learned": 1, "previous_w": 2}
 BC_OUTFLOW, BC_FIXED, BC_NOZZLE = 0, 1, 2
 FACE = {"xlo": 0, "xhi": 1, "ylo": 2, "yhi": 3, "zlo": 4, "zhi": 5}
-CNT_C2P_FAIL, CNT_C2P_FALLBACK, CNT_C2P_ITERS, CNT_C2P_CELLS, CNT_TIMEOUT, CNT_BAD_INDEX = range(6)
+CNT_C2P_FAIL, CNT_C2P_FALLBACK, CNT_C2P_ITERS, CNT_C2P_CELLS, CNT_TIMEOUT, CNT_BAD_INDEX, CNT_C2P_FP64 = range(7)
 CNT_N = 8
 
 
@@ -37,7 +37,8 @@ class VBOptions(C.Structure):
         ("floor_", C.c_double),
         ("w_rtol", C.c_double),
         ("w_max_newton", C.c_int32),
-        ("reserved_i", C.c_int32 * 7),
+        ("c2p_fp32", C.c_int32),
+        ("reserved_i", C.c_int32 * 6),
         ("reserved_d", C.c_double * 4),
     ]
 

@@ -39,6 +39,7 @@ def _sig():
         "vb_batch_get_counters": [vp, C.POINTER(C.c_uint64), vp],
         "vb_batch_reset_counters": [vp, vp],
         "vb_batch_check": [vp, vp],
+        "vb_batch_set_boundary": [vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_int],
         "vb_batch_set_wait_limit": [vp, C.c_uint32],
         "vb_batch_num_variants": [C.c_int],
         "vb_batch_variant_shape": [C.c_int, C.c_int, ip, ip, ip],
@@ -149,6 +150,15 @@ class Batch:
 
     def reset_counters(self, stream=None):
         _chk(self.lib.vb_batch_reset_counters(self._h, _stream_ptr(stream)), self._h)
+
+    def set_boundary(self, i: int, face, kind: int, params=()):
+        """vb_batch_set_boundary: face (0 x-lo, 1 x-hi, 2 y-lo, 3 y-hi or a name
+        of verona_b200._lib.FACE) of problem i gets kind OUTFLOW (0), FIXED (1,
+        params: none or {var, t_on, t_off, factor}) or NOZZLE (2, params:
+        {radius, c1, c2, rho, u, u1[, u2]})."""
+        face = L.FACE[face] if isinstance(face, str) else face
+        par = (C.c_double * 8)(*[float(x) for x in params])
+        _chk(self.lib.vb_batch_set_boundary(self._h, int(i), int(face), int(kind), par, len(params)), self._h)
 
     def check(self, stream=None) -> int:
         """vb_batch_check: synchronises and returns its status code (0, or

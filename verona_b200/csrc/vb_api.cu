@@ -63,6 +63,8 @@ struct vb_solver {
     const void* mlp_blob = nullptr;
     unsigned int* tc_err = nullptr;
     float* w_guess = nullptr;  // one W guess per padded cell
+    unsigned int* defer_idx = nullptr;  // gated learned con2prim: cells left to FP64 (one slot per interior cell)
+    unsigned int* defer_n = nullptr;    // their count
     // asynchronous dumps (vb_dump_begin / vb_dump_wait)
     double* dump_buf = nullptr;            // interior snapshot, reference interior layout
     unsigned long long* dump_nan = nullptr;  // device NaN count of the snapshot
@@ -138,6 +140,7 @@ int vb_default_options(vb_options* o) {
     o->floor_ = 1e-7;
     o->w_rtol = 1e-12;
     o->w_max_newton = 8;
+    o->c2p_fp32 = 1;
     return VB_OK;
 }
 
@@ -158,6 +161,8 @@ int vb_destroy(vb_handle h) {
     cudaFree(h->staging);
     cudaFree(h->tc_err);
     cudaFree(h->w_guess);
+    cudaFree(h->defer_idx);
+    cudaFree(h->defer_n);
     if (h->dump_stream) cudaStreamSynchronize(h->dump_stream);
     cudaFree(h->dump_buf);
     cudaFree(h->dump_nan);
@@ -193,8 +198,10 @@ int vb_create(vb_handle* out, int dims, int nx, int ny, int nz, int nghost, cons
     if (opt.precision < 0 || opt.precision > 1)
         return fail(nullptr, VB_ERR_ARG, "vb_create: precision %d", opt.precision);
     if (opt.n_iter < 1 || opt.n_iter > 100000) return fail(nullptr, VB_ERR_ARG, "vb_create: n_iter %d", opt.n_iter);
-    if (opt.guess == VB_GUESS_LEARNED && dims != 3)
-        return fail(nullptr, VB_ERR_UNSUPPORTED, "vb_create: the learned con2prim guess is provided for 3D grids");
+    if (opt.guess < VB_GUESS_PREVIOUS || opt.guess > VB_GUESS_PREVIOUS_W)
+        return fail(nullptr, VB_ERR_ARG, "vb_create: guess %d", opt.guess);
+    if (opt.guess != VB_GUESS_PREVIOUS && dims != 3)
+        return fail(nullptr, VB_ERR_UNSUPPORTED, "vb_create: the W-Newton con2prim guesses are provided for 3D grids");
     if (nghost == 0 && (opt.riemann != VB_RIEMANN_HLL || opt.rk != 2 || opt.precision != VB_PREC_FP64))
         return fail(nullptr, VB_ERR_UNSUPPORTED,
                     "vb_create: the 1D reference layout (nghost=0) runs the reference scheme only (HLL, RK2, FP64)");
@@ -552,10 +559,12 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
     p.tol = h->opt.tol;
     p.n_iter = h->opt.n_iter;
     p.stats = h->opt.stats;
-    p.c2p_mode = h->opt.guess == VB_GUESS_LEARNED ? C2P_GUESS_W : C2P_REFERENCE;
+    const bool w_newton = h->opt.guess == VB_GUESS_LEARNED || h->opt.guess == VB_GUESS_PREVIOUS_W;
+    p.c2p_mode = w_newton ? C2P_GUESS_W : C2P_REFERENCE;
     p.w_rtol = h->opt.w_rtol;
     p.w_max_newton = h->opt.w_max_newton;
     p.w_guess = nullptr;
+    p.c2p_fp32 = fp32(h) && w_newton && h->opt.c2p_fp32 == 1;
     p.counters = h->cnt;
     p.force_box = h->tun.force_box;
     p.split = h->tun.split_con2prim < 0 ? default_split(h) : h->tun.split_con2prim;
@@ -618,8 +627,19 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
             q.c2p_mode = C2P_GUESS_W;
             q.div_in_pout = stage_div_in_pout<R>(h->dims, h->opt.recon, h->opt.riemann, p);
             if (h->tun.learned_fused != 0) {
-                VB_CUDA(h, launch_c2p_learned<R>(h->mlp_blob, q, bufs, h->tc_err, s));
-                h->launches += 1;
+                if (q.c2p_fp32 && h->defer_idx) {
+                    // precision-gated: FP32 in the fused kernel, the rest by the FP64 pass
+                    q.defer_idx = h->defer_idx;
+                    q.defer_n = h->defer_n;
+                    q.defer_w0 = h->w_guess;
+                    VB_CUDA(h, cudaMemsetAsync(h->defer_n, 0, sizeof(unsigned int), s));
+                    VB_CUDA(h, launch_c2p_learned<R>(h->mlp_blob, q, bufs, h->tc_err, s));
+                    VB_CUDA(h, launch_c2p_deferred<R>(q, bufs, s));
+                    h->launches += 2;
+                } else {
+                    VB_CUDA(h, launch_c2p_learned<R>(h->mlp_blob, q, bufs, h->tc_err, s));
+                    h->launches += 1;
+                }
             } else {
                 VB_CUDA(h, launch_mlp_guess(h->mlp_blob, p, Uo, h->w_guess, h->tc_err, s));
                 q.w_guess = h->w_guess;
@@ -760,6 +780,12 @@ int vb_attach_mlp(vb_handle h, vb_mlp_handle m) {
         int rc = dev_alloc(h, (void**)&h->w_guess, sizeof(float) * (size_t)h->vs);
         if (rc) return rc;
     }
+    if (!h->defer_idx) {
+        const size_t cells = (size_t)h->n[0] * h->n[1] * h->n[2];
+        int rc = dev_alloc(h, (void**)&h->defer_idx, sizeof(unsigned int) * cells);
+        if (!rc) rc = dev_alloc(h, (void**)&h->defer_n, sizeof(unsigned int));
+        if (rc) return rc;
+    }
     if (!h->tc_err) {
         int rc = dev_alloc(h, (void**)&h->tc_err, sizeof(unsigned int));
         if (rc) return rc;
@@ -827,6 +853,15 @@ int vb_point_c2p_w(double gamma, const double* U, const double* W0, double rtol,
         return fail(nullptr, VB_ERR_ARG, "vb_point_c2p_w: bad argument");
     VB_CUDA(nullptr, launch_point_c2p_w(gamma, U, W0, rtol, max_newton, max_bracket, P, iters, fallback, n,
                                         (cudaStream_t)stream));
+    return VB_OK;
+}
+
+int vb_point_c2p_gated(double gamma, const double* U, const float* W0, double rtol, int max_newton, int max_bracket,
+                       double* P, int* iters, int* fp64, int n, void* stream) {
+    if (!U || !W0 || !P || n < 0 || max_newton < 0 || max_bracket < 0 || !(rtol > 0))
+        return fail(nullptr, VB_ERR_ARG, "vb_point_c2p_gated: bad argument");
+    VB_CUDA(nullptr, launch_point_c2p_gated(gamma, U, W0, rtol, max_newton, max_bracket, P, iters, fp64, n,
+                                            (cudaStream_t)stream));
     return VB_OK;
 }
 

@@ -48,6 +48,8 @@ struct vb_batch {
     int ck_cur = 0;
     std::vector<double> ck_t;
     bool has_ck = false;
+    double* dtime = nullptr;    // per problem: its time, on the device (the decay windows of FIXED faces)
+    double* ck_time = nullptr;  // checkpoint of dtime
     unsigned long long* done = nullptr;
     unsigned long long* next = nullptr;
     unsigned long long* cnt = nullptr;
@@ -169,6 +171,7 @@ template <typename R> static BatchLaunch<R> launch_desc(vb_batch_handle b, int n
     a.P1 = (R*)b->P[1];
     a.U0 = b->U[0];
     a.U1 = b->U[1];
+    a.time = b->dtime;
     a.done = b->done;
     a.next = b->next;
     a.counters = b->cnt;
@@ -202,6 +205,7 @@ static int graph_for(vb_batch_handle b, int nsteps, int cur0, cudaGraphExec_t* o
     if (e == cudaSuccess)
         e = b->fp32() ? launch_any<float>(b, nsteps, cur0, b->cap, true)
                       : launch_any<double>(b, nsteps, cur0, b->cap, true);
+    if (e == cudaSuccess) e = batch_advance_time(b->dprob, b->dtime, (int)b->probs.size(), nsteps, b->cap);
     cudaGraph_t graph = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(b->cap, &graph);
     if (e != cudaSuccess || e2 != cudaSuccess) {
@@ -237,6 +241,8 @@ int vb_batch_destroy(vb_batch_handle b) {
     cudaFree(b->ckU);
     cudaFree(b->dprob);
     cudaFree(b->dtiles);
+    cudaFree(b->dtime);
+    cudaFree(b->ck_time);
     cudaFree(b->done);
     cudaFree(b->next);
     cudaFree(b->cnt);
@@ -302,6 +308,7 @@ int vb_batch_create(vb_batch_handle* out, int nprob, const vb_batch_problem* pro
         h.dtdx[1][0] = dth / q.dx;
         h.dtdx[0][1] = q.dims == 2 ? q.dt / q.dy : 0.0;
         h.dtdx[1][1] = q.dims == 2 ? dth / q.dy : 0.0;
+        h.dt = q.dt;  // every face outflow (bc_kind 0) until vb_batch_set_boundary
         b->cells += (long long)q.nx * q.ny;
     }
     b->pool = off;
@@ -310,6 +317,7 @@ int vb_batch_create(vb_batch_handle* out, int nprob, const vb_batch_problem* pro
     if ((rc = balloc(b, &b->P[0], pb)) || (rc = balloc(b, &b->P[1], pb)) || (rc = balloc(b, (void**)&b->U[0], ub)) ||
         (rc = balloc(b, (void**)&b->U[1], ub)) || (rc = balloc(b, (void**)&b->dprob, sizeof(BatchProb) * nprob)) ||
         (rc = balloc(b, (void**)&b->done, sizeof(unsigned long long) * nprob)) ||
+        (rc = balloc(b, (void**)&b->dtime, sizeof(double) * nprob)) ||
         (rc = balloc(b, (void**)&b->next, sizeof(unsigned long long))) ||
         (rc = balloc(b, (void**)&b->cnt, sizeof(unsigned long long) * CNT_N))) {
         g_berr = b->err;
@@ -321,6 +329,7 @@ int vb_batch_create(vb_batch_handle* out, int nprob, const vb_batch_problem* pro
     if (e == cudaSuccess) e = cudaMemset(b->U[0], 0, ub);
     if (e == cudaSuccess) e = cudaMemset(b->U[1], 0, ub);
     if (e == cudaSuccess) e = cudaMemset(b->cnt, 0, sizeof(unsigned long long) * CNT_N);
+    if (e == cudaSuccess) e = cudaMemset(b->dtime, 0, sizeof(double) * nprob);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         g_berr = std::string("vb_batch_create: ") + cudaGetErrorString(e);
@@ -347,6 +356,7 @@ int vb_batch_load_prims(vb_batch_handle b, int i, const double* P_aos, void* str
         BCUDA(b, launch_load_prims<double>(g, P_aos, (double*)b->P[b->cur] + b->off[i], b->U[0] + b->off[i], b->gamma,
                                            s));
     b->t[i] = 0.0;
+    BCUDA(b, cudaMemsetAsync(b->dtime + i, 0, sizeof(double), s));
     return VB_OK;
 }
 
@@ -371,13 +381,39 @@ int vb_batch_step(vb_batch_handle b, int nsteps, void* stream) {
     if (rc) return rc;
     BCUDA(b, cudaGraphLaunch(g, (cudaStream_t)stream));
     if (b->opt.rk == VB_RK3 && (nsteps & 1)) b->cur ^= 1;
-    for (size_t i = 0; i < b->probs.size(); ++i) b->t[i] += nsteps * b->probs[i].dt;
+    // t += dt once per step, as the single-grid solver and the device time advance it
+    for (size_t i = 0; i < b->probs.size(); ++i)
+        for (int k = 0; k < nsteps; ++k) b->t[i] += b->probs[i].dt;
     return VB_OK;
 }
 
 int vb_batch_get_time(vb_batch_handle b, int i, double* t) {
     if (!b || !t || i < 0 || i >= (int)b->probs.size()) return bfail(b, VB_ERR_ARG, "vb_batch_get_time: argument");
     *t = b->t[i];
+    return VB_OK;
+}
+
+int vb_batch_set_boundary(vb_batch_handle b, int i, int face, int kind, const double* par, int np) {
+    if (!b) return bfail(nullptr, VB_ERR_ARG, "null batch");
+    if (i < 0 || i >= (int)b->probs.size()) return bfail(b, VB_ERR_ARG, "vb_batch_set_boundary: problem %d", i);
+    const int dims = b->probs[i].dims, nv = 2 + dims;
+    if (face < 0 || face >= 2 * dims)
+        return bfail(b, VB_ERR_ARG, "vb_batch_set_boundary: face %d for dims %d", face, dims);
+    if (kind < 0 || kind > 2) return bfail(b, VB_ERR_ARG, "vb_batch_set_boundary: kind %d", kind);
+    if (np < 0 || np > 8 || (np > 0 && !par)) return bfail(b, VB_ERR_ARG, "vb_batch_set_boundary: %d params", np);
+    if (kind == VB_BC_FIXED && np > 0 && np < 4)
+        return bfail(b, VB_ERR_ARG, "vb_batch_set_boundary: FIXED decay needs {var, t_on, t_off, factor}");
+    if (kind == VB_BC_FIXED && np >= 4 && (par[0] < 0 || par[0] >= nv))
+        return bfail(b, VB_ERR_ARG, "vb_batch_set_boundary: decay variable %g", par[0]);
+    if (kind == VB_BC_NOZZLE && np < 5 + dims)
+        return bfail(b, VB_ERR_ARG, "vb_batch_set_boundary: NOZZLE needs {radius, c1, c2, rho, u, u1..u%d}", dims);
+    BatchProb& h = b->hp[i];
+    h.bc_kind[face] = kind;
+    for (int k = 0; k < 8; ++k) h.bc_par[face][k] = k < np ? par[k] : 0.0;
+    if (kind == VB_BC_FIXED && np == 0) h.bc_par[face][0] = -1.0;  // no decay
+    // the descriptor is read by launches already queued: replace it in order
+    BCUDA(b, cudaDeviceSynchronize());
+    BCUDA(b, cudaMemcpy(b->dprob + i, &h, sizeof(BatchProb), cudaMemcpyHostToDevice));
     return VB_OK;
 }
 
@@ -460,14 +496,17 @@ int vb_batch_info(vb_batch_handle b, int64_t* interior_cells, int64_t* tiles_per
 int vb_batch_checkpoint(vb_batch_handle b, void* stream) {
     if (!b) return bfail(nullptr, VB_ERR_ARG, "null batch");
     const size_t pb = b->psize() * (size_t)b->pool, ub = sizeof(double) * (size_t)b->pool;
+    const size_t tb = sizeof(double) * b->probs.size();
     if (!b->ckP) {
         int rc = balloc(b, &b->ckP, pb);
         if (!rc) rc = balloc(b, (void**)&b->ckU, ub);
+        if (!rc) rc = balloc(b, (void**)&b->ck_time, tb);
         if (rc) return rc;
     }
     cudaStream_t s = (cudaStream_t)stream;
     BCUDA(b, cudaMemcpyAsync(b->ckP, b->P[b->cur], pb, cudaMemcpyDeviceToDevice, s));
     BCUDA(b, cudaMemcpyAsync(b->ckU, b->U[0], ub, cudaMemcpyDeviceToDevice, s));
+    BCUDA(b, cudaMemcpyAsync(b->ck_time, b->dtime, tb, cudaMemcpyDeviceToDevice, s));
     b->ck_cur = b->cur;
     b->ck_t = b->t;
     b->has_ck = true;
@@ -482,6 +521,7 @@ int vb_batch_rollback(vb_batch_handle b, void* stream) {
     b->cur = b->ck_cur;
     BCUDA(b, cudaMemcpyAsync(b->P[b->cur], b->ckP, pb, cudaMemcpyDeviceToDevice, s));
     BCUDA(b, cudaMemcpyAsync(b->U[0], b->ckU, ub, cudaMemcpyDeviceToDevice, s));
+    BCUDA(b, cudaMemcpyAsync(b->dtime, b->ck_time, sizeof(double) * b->probs.size(), cudaMemcpyDeviceToDevice, s));
     b->t = b->ck_t;
     return VB_OK;
 }

@@ -40,20 +40,33 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
     return v;
 }
 
-// ghost layers read by one tile: x-ghosts of its rows on an x edge, y-ghosts
-// of its columns on a y edge
+// Ghost layers read by one tile: x-ghosts of its rows on an x edge, y-ghosts
+// of its columns on a y edge. At the first stage of a step (first) they are
+// filled as the single-grid solver fills them at the start of the step
+// (vb_set_boundary kinds, launch_bc_face / launch_bc_decay): OUTFLOW copies
+// the first interior cell, NOZZLE holds the inflow state inside the radius
+// (cells measured from the centre along the face) and copies outside it,
+// FIXED keeps the loaded ghosts and multiplies the decaying variable by its
+// factor while t_on < t < t_off (t: the problem's time at the start of the
+// step). The stage output gets the floored ghosts (k_ghost_limit); later
+// stages copy the floored ghosts of their input.
 template <typename R>
-__device__ __forceinline__ void batch_ghosts(const StageParams& q, const R* Pin_c, R* Pout, int dims, int nv,
-                                             int bx, int by, int ntx, int nty, int TXc, int TYc, bool first) {
+__device__ __forceinline__ void batch_ghosts(const StageParams& q, const BatchProb& pr, const R* Pin_c, R* Pout,
+                                             int bx, int by, int TXc, int TYc, bool first, double t) {
     R* Pin = const_cast<R*>(Pin_c);
+    const int dims = pr.dims, nv = 2 + dims;
     const R fl = R(q.floor_);
     const int n0 = q.n[0], n1 = q.n[1];
     const int ox = NG + bx * TXc, oy = dims > 1 ? NG + by * TYc : 0;
     const int vx = min(TXc, n0 - NG - ox), vy = dims > 1 ? min(TYc, n1 - NG - oy) : 1;
     // up to four edges: x-lo, x-hi (rows oy..oy+vy), y-lo, y-hi (columns ox..ox+vx)
     for (int edge = 0; edge < 4; ++edge) {
-        const bool on = edge == 0 ? bx == 0 : edge == 1 ? bx == ntx - 1 : dims > 1 && (edge == 2 ? by == 0 : by == nty - 1);
+        const bool on =
+            edge == 0 ? bx == 0 : edge == 1 ? bx == pr.ntx - 1 : dims > 1 && (edge == 2 ? by == 0 : by == pr.nty - 1);
         if (!on) continue;
+        const int kind = pr.bc_kind[edge];
+        const double* par = pr.bc_par[edge];
+        const int dvar = first && kind == 1 && par[0] >= 0.0 && t > par[1] && t < par[2] ? (int)par[0] : -1;
         const int len = edge < 2 ? vy : vx;
         for (int e = threadIdx.x; e < NG * len; e += blockDim.x) {
             const int layer = e / len, r = e - layer * len;
@@ -69,10 +82,29 @@ __device__ __forceinline__ void batch_ghosts(const StageParams& q, const R* Pin_
                 gj = edge == 2 ? layer : n1 - NG + layer;
                 sj = edge == 2 ? NG : n1 - NG - 1;
             }
+            bool inside = false;
+            if (kind == 2) {
+                const double y1 = dims > 1 ? ((edge < 2 ? gj : gi) - NG + 0.5) - par[1] : 0.0;
+                inside = y1 * y1 < par[0] * par[0];
+            }
             const long long c = gi + q.sy * gj, cs = si + q.sy * sj;
             for (int v = 0; v < nv; ++v) {
-                R x = __ldcg(Pin + v * q.vs + (first ? cs : c));
-                if (first) Pin[v * q.vs + c] = x;
+                R x;
+                if (!first) {
+                    x = __ldcg(Pin + v * q.vs + c);
+                } else if (kind == 1) {
+                    x = __ldcg(Pin + v * q.vs + c);
+                    if (v == dvar) {
+                        x = (R)((double)x * par[3]);
+                        Pin[v * q.vs + c] = x;
+                    }
+                } else if (inside) {
+                    x = (R)par[v < 2 ? 3 + v : 5 + (v - 2)];
+                    Pin[v * q.vs + c] = x;
+                } else {
+                    x = __ldcg(Pin + v * q.vs + cs);
+                    Pin[v * q.vs + c] = x;
+                }
                 if (v < 2) x = jmax(x, fl);
                 Pout[v * q.vs + c] = x;
             }
@@ -161,7 +193,11 @@ __global__ void __launch_bounds__(BATCH_NT) k_batch(BatchLaunch<R> a) {
         b.U0 = U0;
 
         const int TXc = pr.dims == 1 ? L1 : TX2, TYc = pr.dims == 1 ? 1 : TY2;
-        batch_ghosts<R>(q, b.Pin, b.Pout, pr.dims, 2 + pr.dims, e.x, e.y, pr.ntx, pr.nty, TXc, TYc, st == 0);
+        // the problem's time at the start of this step: its time at the start
+        // of the launch plus dt once per earlier step (the host's additions)
+        double tstep = a.time[e.p];
+        for (int k = 0; k < step; ++k) tstep += pr.dt;
+        batch_ghosts<R>(q, pr, b.Pin, b.Pout, e.x, e.y, TXc, TYc, st == 0, tstep);
         __threadfence_block();
         __syncthreads();
         if (pr.dims == 1) {

@@ -19,6 +19,11 @@ struct BatchProb {
     long long offP, offU;   // element offset of variable 0 in the P / U pools
     long long vs;           // variable stride
     double dtdx[2][2];      // [full dt, half dt (RK2 stage 1)][axis]
+    double dt;              // time step (the time of a step for a decaying FIXED face)
+    int bc_kind[4];         // per face x-lo, x-hi, y-lo, y-hi: 0 outflow, 1 fixed, 2 nozzle (VB_BC_*)
+    int bc_pad;
+    double bc_par[4][8];    // FIXED {var (< 0: no decay), t_on, t_off, factor}; NOZZLE {radius, c1, c2,
+                            // rho, u, u1[, u2]} (vb_set_boundary's parameters)
 };
 
 struct BatchTile {
@@ -36,6 +41,7 @@ template <typename R> struct BatchLaunch {
     R* P1;
     double* U0;
     double* U1;
+    const double* time;        // per problem: its time at the start of the launch
     unsigned long long* done;  // per problem
     unsigned long long* next;  // ticket counter
     unsigned long long* counters;
@@ -49,6 +55,9 @@ template <typename R> struct BatchLaunch {
 template <typename R>
 cudaError_t batch_launch(const BatchLaunch<R>& a, int riemann, int variant, int ctas_per_sm, cudaStream_t s,
                          int* grid, bool launch);
+// advance every problem's device time by nsteps steps (t += dt, one step at a
+// time, the same additions the host makes); the graph's last node
+cudaError_t batch_advance_time(const BatchProb* prob, double* time, int nprob, int nsteps, cudaStream_t s);
 // number of tile-shape variants and the shape of one: 2D tile TX2 x TY2, 1D pencil L1
 template <typename R> int batch_num_variants();
 template <typename R> void batch_variant_shape(int v, int* tx2, int* ty2, int* l1);

@@ -571,4 +571,182 @@ VB_HD int c2p_w(double g, const double* Uc, double W0, double rtol, int max_newt
     return -(it + 1);
 }
 
+// ---- precision-gated con2prim of the FP32-bulk form ----------------------------
+// In the FP32-bulk form the recovered primitives are stored in FP32 and feed
+// only the FP32 reconstruction; U and the RK accumulation stay FP64. Where the
+// inversion U -> P is well conditioned an FP32 Newton is enough, and FP64 is
+// kept for the cells where it is not: high Lorentz factor (1 - v^2 loses
+// digits) and cold moving gas (p is then a small difference of kinetic and
+// total energy). The FP32 Newton solves for the pressure with a residual free
+// of O(D) - O(D) cancellations: with E = D + tau (tau = E - D formed in FP64),
+// W = E + p, v^2 = S^2 / W^2, s = sqrt(1 - v^2) and k' = Gamma / (Gamma - 1),
+//   f(p) = (tau + p)(1 - v^2) - k' p - D v^2 s / (1 + s)
+// (the W residual of the 1DW scheme, src/3dim/structs.jl:273-343, divided by
+// -k = -(Gamma - 1) / Gamma, with D (1 - v^2) - D s rewritten as
+// -D v^2 s / (1 + s)),
+//   f'(p) = (1 - v^2) + (tau + p) 2 v^2 / W - k' + D h'(v^2) 2 v^2 / W,
+//   h'(v^2) = s / (1 + s) - v^2 / (2 s (1 + s)^2).
+// Gate: p0 > 0, v^2 < 1/2 (Lorentz factor below sqrt 2) and v^2 D < 10 p
+// (kinetic over thermal energy below about 10), checked on the guess and
+// again on the converged pressure (a W guess a little off can put p0 far
+// above a cold gas's pressure); a cell that fails either check, or whose
+// Newton does not converge in C2P32_MAX_IT steps, goes to the FP64 W Newton.
+// The reciprocals and the reciprocal square root are the sm_100a hardware
+// approximations (relative error below 2^-22, as FP32 rounding), four per
+// iteration; the Newton stops once a step is below 1e-5 of p, where its
+// quadratic convergence leaves an error far below FP32 rounding. Every
+// operation is an explicit instruction (inline PTX or a round-to-nearest
+// intrinsic), so the result does not depend on the contraction or division
+// flags of the translation unit: the fused and the two-kernel learned forms
+// agree bit for bit.
+constexpr float C2P32_MAX_V2 = 0.5f;
+constexpr float C2P32_MAX_KIN = 10.0f;
+constexpr float C2P32_RTOL = 1e-5f;
+constexpr int C2P32_MAX_IT = 6;
+
+#ifdef __CUDA_ARCH__
+VB_HD float f_add(float a, float b) { return __fadd_rn(a, b); }
+VB_HD float f_sub(float a, float b) { return __fsub_rn(a, b); }
+VB_HD float f_mul(float a, float b) { return __fmul_rn(a, b); }
+VB_HD float f_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+VB_HD float f_rcp(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+VB_HD float f_rsqrt(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+#else
+VB_HD float f_add(float a, float b) { return a + b; }
+VB_HD float f_sub(float a, float b) { return a - b; }
+VB_HD float f_mul(float a, float b) { return a * b; }
+VB_HD float f_fma(float a, float b, float c) { return fmaf(a, b, c); }
+VB_HD float f_rcp(float x) { return 1.0f / x; }
+VB_HD float f_rsqrt(float x) { return 1.0f / sqrtf(x); }
+#endif
+
+// The conserved state of one cell as the FP32 Newton sees it.
+struct C2P32In {
+    float D, tau, E, S2, Sx, Sy, Sz;
+};
+
+// the gate's conditions at pressure p with v^2 = S^2 / W^2
+VB_HD bool c2p32_admits(const C2P32In& in, float v2, float p) {
+    return v2 < C2P32_MAX_V2 && f_mul(v2, in.D) < f_mul(C2P32_MAX_KIN, p);
+}
+
+// Gate of the FP32 solve from the guess W0 (FP32, the learned guess as both
+// learned forms round it): true, with the FP32 inputs and the pressure guess
+// p0, when the cell qualifies.
+VB_HD bool c2p32_gate(const double* U, float W0, C2P32In& in, float& p0) {
+    const double E = -U[1];
+    const double S2 = U[2] * U[2] + U[3] * U[3] + U[4] * U[4];
+    p0 = (float)((double)W0 - E);
+    in.D = (float)U[0];
+    in.tau = (float)(E - U[0]);
+    in.E = (float)E;
+    in.S2 = (float)S2;
+    in.Sx = (float)U[2];
+    in.Sy = (float)U[3];
+    in.Sz = (float)U[4];
+    if (!(p0 > 0.0f) || !(W0 > 0.0f) || !(in.D > 0.0f) || !(in.tau > 0.0f)) return false;
+    const float iW = f_rcp(W0);
+    return c2p32_admits(in, f_mul(f_mul(in.S2, iW), iW), p0);
+}
+
+// FP32 Newton on the pressure from p0; returns the iterations on convergence
+// (a step below C2P32_RTOL p, and the gate holding at the root), else
+// -C2P32_MAX_IT.
+VB_HD int c2p_p32(float g, const C2P32In& in, float p0, float& p_out) {
+    const float kp = f_mul(g, f_rcp(f_sub(g, 1.0f)));
+    float p = p0;
+    for (int it = 1; it <= C2P32_MAX_IT; ++it) {
+        const float iW = f_rcp(f_add(in.E, p));
+        const float v2 = f_mul(f_mul(in.S2, iW), iW);
+        const float a = f_sub(1.0f, v2);
+        if (!(a > 0.0f)) return -C2P32_MAX_IT;
+        const float rs = f_rsqrt(a);          // 1 / s
+        const float sr = f_mul(a, rs);        // s
+        const float q = f_rcp(f_add(1.0f, sr));
+        const float h = f_mul(sr, q);         // s / (1 + s)
+        const float tp = f_add(in.tau, p);
+        const float Dv2 = f_mul(in.D, v2);
+        // f = tp a - k' p - D v^2 h
+        const float f = f_sub(f_fma(tp, a, f_mul(-kp, p)), f_mul(Dv2, h));
+        const float dv2 = f_mul(-2.0f, f_mul(v2, iW));  // d v^2 / dp
+        // h'(v^2) = h - v^2 q^2 / (2 s)
+        const float dh = f_sub(h, f_mul(f_mul(f_mul(0.5f, v2), f_mul(q, q)), rs));
+        const float df = f_sub(f_sub(f_fma(-tp, dv2, a), kp), f_mul(f_mul(in.D, dh), dv2));
+        const float dp = f_mul(f, f_rcp(df));
+        float pn = f_sub(p, dp);
+        if (!(pn > 0.0f)) pn = f_mul(0.5f, p);
+        const bool done = fabsf(f_sub(pn, p)) <= f_mul(C2P32_RTOL, pn);
+        p = pn;
+        if (done) {
+            const float iWn = f_rcp(f_add(in.E, p));
+            if (!c2p32_admits(in, f_mul(f_mul(in.S2, iWn), iWn), p)) return -C2P32_MAX_IT;
+            p_out = p;
+            return it;
+        }
+    }
+    return -C2P32_MAX_IT;
+}
+
+// Primitives from the converged FP32 pressure, with the 3D floors of the
+// reference's final-state formula (src/3dim/structs.jl:598-609).
+VB_HD void prims_from_p32(float g, const C2P32In& in, float p, double* P) {
+    const float iW = f_rcp(f_add(in.E, p));
+    const float v2 = f_mul(f_mul(in.S2, iW), iW);
+    const float a = f_sub(1.0f, v2);
+    const float rs = f_rsqrt(a);   // Lorentz factor (below sqrt 2: no cap)
+    const float fac = f_mul(iW, rs);  // Lorentz factor / W
+    P[0] = (double)fmaxf(1e-8f, f_mul(in.D, f_mul(a, rs)));
+    P[1] = (double)fmaxf(1e-8f, f_mul(p, f_rcp(f_sub(g, 1.0f))));
+    P[2] = (double)f_mul(in.Sx, fac);
+    P[3] = (double)f_mul(in.Sy, fac);
+    P[4] = (double)f_mul(in.Sz, fac);
+}
+
+// The learned guess's refinement with the precision gate: the FP32 pressure
+// Newton where c2p32_gate admits the cell (and it converges), else the FP64 W
+// Newton with its bracketed fallback (c2p_w). *fp64 = 1 where the FP64 Newton
+// ran. Returns the iterations (negative on failure).
+VB_HD int c2p_w_gated(double g, const double* U, float W0f, double rtol, int max_newton, int max_bracket, bool gate,
+                      double* P, int* used_fallback, int* fp64) {
+    if (gate) {
+        C2P32In in;
+        float p0;
+        if (c2p32_gate(U, W0f, in, p0)) {
+            float pp;
+            const int r = c2p_p32((float)g, in, p0, pp);
+            if (r > 0) {
+                prims_from_p32((float)g, in, pp, P);
+                *used_fallback = 0;
+                *fp64 = 0;
+                return r;
+            }
+        }
+    }
+    *fp64 = 1;
+    return c2p_w(g, U, (double)W0f, rtol, max_newton, max_bracket, P, used_fallback);
+}
+
+// The FP32 part of c2p_w_gated alone: true, with the primitives in P and the
+// iterations in *iters, when the gate admits the cell and the FP32 Newton
+// converges; false when the cell needs the FP64 W Newton.
+VB_HD bool c2p_try_fp32(double g, const double* U, float W0f, double* P, int* iters) {
+    C2P32In in;
+    float p0;
+    if (!c2p32_gate(U, W0f, in, p0)) return false;
+    float pp;
+    const int r = c2p_p32((float)g, in, p0, pp);
+    if (r <= 0) return false;
+    prims_from_p32((float)g, in, pp, P);
+    *iters = r;
+    return true;
+}
+
 }  // namespace vb

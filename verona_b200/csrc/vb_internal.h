@@ -16,6 +16,7 @@ enum Counter {
     CNT_C2P_CELLS = 3,     // cells solved (statistics mode only)
     CNT_TIMEOUT = 4,       // a bounded wait in a persistent kernel gave up
     CNT_BAD_INDEX = 5,     // a work item outside its bounds was skipped
+    CNT_C2P_FP64 = 6,      // cells solved by the FP64 Newton of the gated learned refinement (statistics mode)
     CNT_N = 8
 };
 
@@ -35,6 +36,11 @@ struct StageParams {
     double w_rtol;       // C2P_GUESS_W: relative tolerance of the W Newton
     int w_max_newton;    // C2P_GUESS_W: Newton steps before the bracketed fallback
     const float* w_guess;  // C2P_GUESS_W: per-cell W guesses (nullptr: derive from Pin)
+    int c2p_fp32;        // C2P_GUESS_W from learned guesses: precision-gated refinement (c2p_w_gated)
+    unsigned int* defer_idx;  // gated fused learned con2prim: interior indices of the cells left to the FP64
+                              //    W Newton (capacity: every interior cell), their count in *defer_n and
+    unsigned int* defer_n;    //    their FP32 W guesses in defer_w0 (per padded cell); solved by
+    float* defer_w0;          //    launch_c2p_deferred after the fused kernel
     unsigned long long* counters;
     int force_box;       // 1: use the box-tile kernel even where the z-marching one fits
     int split;           // 1: z-marching stencil kernel writes U only; k_c2p solves con2prim
@@ -116,8 +122,8 @@ int max_speed_blocks(const Grid& g);
 
 // FP32-bulk z-pair variant of the 3D stage (vb_stage_zp.cuh, instantiated in
 // vb_stage_f32.cu): WENOZ reconstruction with HLL or HLLC
-inline bool zp_available(int rec, int rs) { return rec == 2 && (rs == 0 || rs == 1); }
-cudaError_t launch_stage_zp(int rs, const StageParams& p, const StageBufs<float>& b, cudaStream_t s);
+inline bool zp_available(int rec, int rs) { return rec >= 0 && rec <= 2 && (rs == 0 || rs == 1); }
+cudaError_t launch_stage_zp(int rec, int rs, const StageParams& p, const StageBufs<float>& b, cudaStream_t s);
 // tensor map of one SoA state array for the TMA forms of the stage kernels
 // (3D FP32: the z-pair kernel's plane boxes; 2D: k_stage's tile boxes; out: a
 // 64-byte aligned CUtensorMap); false where no TMA form exists or the layout
@@ -144,6 +150,9 @@ cudaError_t launch_mlp_guess(const void* mlp_blob, const StageParams& p, const d
 template <typename R>
 cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const StageBufs<R>& b, unsigned int* err,
                                cudaStream_t s);
+// the cells the gated fused kernel left (p.defer_idx, *p.defer_n, p.defer_w0):
+// the FP64 W Newton from their guesses, floors, P (vb_mlp.cu)
+template <typename R> cudaError_t launch_c2p_deferred(const StageParams& p, const StageBufs<R>& b, cudaStream_t s);
 
 // point kernels (FP64, vb_stage_f64.cu)
 cudaError_t launch_point_recon(int method, const double* q, double* out, int n, cudaStream_t s);
@@ -153,6 +162,8 @@ cudaError_t launch_point_con2prim(int dims, double g, int n_iter, double tol, co
                                   int n, cudaStream_t s);
 cudaError_t launch_point_c2p_w(double g, const double* U, const double* W0, double rtol, int max_newton,
                                int max_bracket, double* P, int* iters, int* fallback, int n, cudaStream_t s);
+cudaError_t launch_point_c2p_gated(double g, const double* U, const float* W0, double rtol, int max_newton,
+                                   int max_bracket, double* P, int* iters, int* fp64, int n, cudaStream_t s);
 
 }  // namespace vb
 

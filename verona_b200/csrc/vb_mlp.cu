@@ -827,7 +827,12 @@ cudaError_t launch_mlp_guess(const void* mlp_blob, const StageParams& p, const d
 // divergence in Pout, and this kernel forms U = rk_a U0 + rk_b (Us - div)
 // (written to Uo) before the features; the next tile's inputs are loaded
 // before the current tile's Newton, whose latency covers them.
-template <typename R>
+// GATED (the precision-gated refinement, options.c2p_fp32): every cell the
+// FP32 gate admits is finished here by the FP32 pressure Newton; the others
+// are appended, with their guess, to a list (one atomic per warp) that
+// k_c2p_deferred solves with the FP64 W Newton after this kernel, so this
+// kernel carries no FP64 Newton and keeps its registers for the network.
+template <typename R, bool GATED>
 __global__ void __launch_bounds__(TILE, 5) k_c2p_learned(const MlpBlob* __restrict__ blob, StageParams p,
                                                          StageBufs<R> b, unsigned int* err) {
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -893,11 +898,38 @@ __global__ void __launch_bounds__(TILE, 5) k_c2p_learned(const MlpBlob* __restri
         if (!mlp_forward_tile(s, f, y, phase, err)) break;
         Raw rn;
         if (okn) load(cn, rn);
-        if (ok) {
-            const double W0 = (double)(float)(-u[1] * (1.0 + (double)fmaxf(y, 0.0f)));
+        // the guess rounded to FP32 exactly as the two-kernel form stores it
+        const float W0 = (float)(-u[1] * (1.0 + (double)fmaxf(y, 0.0f)));
+        if constexpr (GATED) {
+            // FP32 pressure Newton where the gate admits the cell; the rest to the list
+            double P[5];
+            int r = 0;
+            const bool done = ok && c2p_try_fp32(p.gamma, u, W0, P, &r);
+            if (done) {
+                n_it += r;
+                n_cells += 1;
+                P[0] = jmax(P[0], p.floor_);
+                P[1] = jmax(P[1], p.floor_);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) b.Pout[v * vs + c] = (R)P[v];
+            }
+            const bool defer = ok && !done;
+            const unsigned m = __ballot_sync(0xffffffffu, defer);
+            if (m) {
+                const int lane = t & 31, leader = __ffs(m) - 1;
+                unsigned base = 0;
+                if (lane == leader) base = atomicAdd(p.defer_n, (unsigned)__popc(m));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (defer) {
+                    p.defer_idx[base + __popc(m & ((1u << lane) - 1u))] = (unsigned)(tile * TILE + t);
+                    p.defer_w0[c] = W0;
+                }
+            }
+        } else if (ok) {
+            // the FP64 W Newton on every cell
             double P[5];
             int fb;
-            const int r = c2p_w(p.gamma, u, W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, P, &fb);
+            const int r = c2p_w(p.gamma, u, (double)W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, P, &fb);
             n_fail += (r < 0);
             n_fb += fb;
             n_it += (r < 0 ? -r : r);
@@ -925,25 +957,27 @@ __global__ void __launch_bounds__(TILE, 5) k_c2p_learned(const MlpBlob* __restri
             if (n_fb) atomicAdd(cnt + CNT_C2P_FALLBACK, n_fb);
             if (n_it) atomicAdd(cnt + CNT_C2P_ITERS, n_it);
             if (n_cells) atomicAdd(cnt + CNT_C2P_CELLS, n_cells);
+            // ungated: every cell ran the FP64 Newton (gated: k_c2p_deferred counts them)
+            if (!GATED && n_cells) atomicAdd(cnt + CNT_C2P_FP64, n_cells);
         }
     } else if (n_fb) {
         atomicAdd(cnt + CNT_C2P_FALLBACK, n_fb);
     }
 }
 
-template <typename R>
-cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const StageBufs<R>& b, unsigned int* err,
-                               cudaStream_t s) {
+template <typename R, bool GATED>
+cudaError_t launch_c2p_learned_t(const void* mlp_blob, const StageParams& p, const StageBufs<R>& b, unsigned int* err,
+                                 cudaStream_t s) {
     static unsigned long long attr = 0;
     static int resident[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     const int d = dev & 63;
     if (!(attr >> d & 1ULL)) {
-        cudaError_t e = cudaFuncSetAttribute(k_c2p_learned<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_c2p_learned<R, GATED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)sizeof(InferSmem));
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(k_c2p_learned<R>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        e = cudaFuncSetAttribute(k_c2p_learned<R, GATED>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         // 5 CTAs per SM: the launch bound (96 registers x 128 threads), 5 x 43 KB of
         // shared memory and 5 x 64 TMEM columns all fit (the occupancy query
@@ -960,13 +994,91 @@ cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const
     const long long tiles = (cells + TILE - 1) / TILE;
     const int nb = (int)std::min<long long>(tiles, resident[d]);
     if (nb <= 0) return cudaSuccess;
-    k_c2p_learned<R><<<nb, TILE, sizeof(InferSmem), s>>>((const MlpBlob*)mlp_blob, p, b, err);
+    k_c2p_learned<R, GATED><<<nb, TILE, sizeof(InferSmem), s>>>((const MlpBlob*)mlp_blob, p, b, err);
     return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_c2p_learned(const void* mlp_blob, const StageParams& p, const StageBufs<R>& b, unsigned int* err,
+                               cudaStream_t s) {
+    if (p.c2p_fp32 && p.defer_idx && p.defer_n && p.defer_w0)
+        return launch_c2p_learned_t<R, true>(mlp_blob, p, b, err, s);
+    return launch_c2p_learned_t<R, false>(mlp_blob, p, b, err, s);
 }
 template cudaError_t launch_c2p_learned<float>(const void*, const StageParams&, const StageBufs<float>&,
                                                unsigned int*, cudaStream_t);
 template cudaError_t launch_c2p_learned<double>(const void*, const StageParams&, const StageBufs<double>&,
                                                 unsigned int*, cudaStream_t);
+
+// The cells the gated fused kernel left to FP64: the W Newton from their FP32
+// guesses (as the ungated kernel runs it), the floors, P. The count is read on
+// the device, bounded by the list's capacity (every interior cell).
+template <typename R>
+__global__ void __launch_bounds__(256) k_c2p_deferred(StageParams p, StageBufs<R> b) {
+    const int N0 = p.n[0] - 2 * NG, N1 = p.n[1] - 2 * NG, N2 = p.n[2] - 2 * NG;
+    const unsigned long long cap = (unsigned long long)N0 * N1 * N2;
+    const unsigned long long n = std::min<unsigned long long>(*p.defer_n, cap);
+    CellMap cm;  // interior cells < 2^32 (launch_c2p_deferred)
+    cm.init(N0, N1, p.sy, p.sz, NG);
+    const long long vs = p.vs;
+    unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned e = p.defer_idx[i];
+        if ((unsigned long long)e >= cap) {
+            if (p.counters) atomicAdd(p.counters + CNT_BAD_INDEX, 1ULL);
+            continue;
+        }
+        const long long c = cm.padded(e);
+        double U[5], P[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) U[v] = b.Uo[v * vs + c];
+        int fb;
+        const int r = c2p_w(p.gamma, U, (double)p.defer_w0[c], p.w_rtol, p.w_max_newton, 4 * p.n_iter, P, &fb);
+        n_fail += (r < 0);
+        n_fb += fb;
+        n_it += (r < 0 ? -r : r);
+        n_cells += 1;
+        P[0] = jmax(P[0], p.floor_);
+        P[1] = jmax(P[1], p.floor_);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) b.Pout[v * vs + c] = (R)P[v];
+    }
+    unsigned long long* cnt = p.counters;
+    if (!cnt) return;
+    if (n_fail) atomicAdd(cnt + CNT_C2P_FAIL, n_fail);
+    if (p.stats) {
+        for (int o = 16; o > 0; o >>= 1) {
+            n_fb += __shfl_xor_sync(0xffffffffu, n_fb, o);
+            n_it += __shfl_xor_sync(0xffffffffu, n_it, o);
+            n_cells += __shfl_xor_sync(0xffffffffu, n_cells, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            if (n_fb) atomicAdd(cnt + CNT_C2P_FALLBACK, n_fb);
+            if (n_it) atomicAdd(cnt + CNT_C2P_ITERS, n_it);
+            if (n_cells) {
+                atomicAdd(cnt + CNT_C2P_CELLS, n_cells);
+                atomicAdd(cnt + CNT_C2P_FP64, n_cells);
+            }
+        }
+    } else if (n_fb) {
+        atomicAdd(cnt + CNT_C2P_FALLBACK, n_fb);
+    }
+}
+
+template <typename R> cudaError_t launch_c2p_deferred(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
+    const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
+    if ((unsigned long long)cells > MAX_CELLS_U32 || !p.defer_idx || !p.defer_n || !p.defer_w0)
+        return cudaErrorInvalidValue;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int nb = (int)std::max<long long>(1, std::min<long long>((cells + 255) / 256, 8LL * std::max(1, sms)));
+    k_c2p_deferred<R><<<nb, 256, 0, s>>>(p, b);
+    return cudaGetLastError();
+}
+template cudaError_t launch_c2p_deferred<float>(const StageParams&, const StageBufs<float>&, cudaStream_t);
+template cudaError_t launch_c2p_deferred<double>(const StageParams&, const StageBufs<double>&, cudaStream_t);
 }  // namespace vb
 
 extern "C" {

@@ -82,19 +82,37 @@ __device__ __forceinline__ void count_add(unsigned long long* c, int which, unsi
     if (c && v) atomicAdd(c + which, v);
 }
 
+// the learned guess's refinement of one cell (two-kernel learned form), out of
+// line: kernels that run the reference cascade keep its registers out of theirs
+static __device__ __noinline__ int solve_cell_learned(const StageParams& p, const double* U, double* P, float W0,
+                                                      int* fallback, int* fp64) {
+    return c2p_w_gated(p.gamma, U, W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, p.c2p_fp32 != 0, P, fallback, fp64);
+}
+
 // con2prim of one cell: per-dimension reference algorithm, or the W Newton
 // from a supplied guess with the bracketed fallback.
 template <int DIM>
 __device__ __forceinline__ int solve_cell(const StageParams& p, const double* U, double* P, long long gidx,
-                                          int& fallback) {
+                                          int& fallback, int* fp64 = nullptr) {
     fallback = 0;
     if (DIM == 3 && p.c2p_mode == C2P_GUESS_W) {
         double W0;
         if (p.w_guess) {
-            W0 = (double)p.w_guess[gidx];
+            // the learned guess, with the precision gate of the FP32-bulk form
+            int f64 = 1;
+            const int it = solve_cell_learned(p, U, P, p.w_guess[gidx], &fallback, &f64);
+            if (fp64) *fp64 = f64;
+            return it;
         } else {
+            // the previous state's W (VB_GUESS_PREVIOUS_W), with the same gate
             double gm2 = sq(P[2]) + sq(P[3]) + sq(P[4]) + 1.0;
             W0 = (P[0] + p.gamma * P[1]) * gm2;
+            if (p.c2p_fp32) {
+                int f64 = 1;
+                const int it = solve_cell_learned(p, U, P, (float)W0, &fallback, &f64);
+                if (fp64) *fp64 = f64;
+                return it;
+            }
         }
         int fb;
         int it = c2p_w(p.gamma, U, W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, P, &fb);

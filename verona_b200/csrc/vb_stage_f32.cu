@@ -6,8 +6,8 @@
 #include "vb_stage_zp.cuh"
 
 namespace vb {
-cudaError_t launch_stage_zp(int rs, const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
-    return dispatch_stage_zp(rs, p, b, s);
+cudaError_t launch_stage_zp(int rec, int rs, const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
+    return dispatch_stage_zp(rec, rs, p, b, s);
 }
 
 // Tensor maps of an FP32 state array. 3D, for the TMA form of the z-pair

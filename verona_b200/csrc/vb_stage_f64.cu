@@ -106,6 +106,28 @@ cudaError_t launch_point_c2p_w(double g, const double* U, const double* W0, doub
     return cudaGetLastError();
 }
 
+// the learned guess's precision-gated refinement (c2p_w_gated) from FP32 guesses
+__global__ void k_point_c2p_gated(double g, const double* __restrict__ U, const float* __restrict__ W0, double rtol,
+                                  int max_newton, int max_bracket, double* __restrict__ P, int* __restrict__ iters,
+                                  int* __restrict__ fp64, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double u[5], p[5];
+        for (int v = 0; v < 5; ++v) u[v] = U[v * n + i];
+        int fb = 0, f64 = 1;
+        int r = c2p_w_gated(g, u, W0[i], rtol, max_newton, max_bracket, true, p, &fb, &f64);
+        for (int v = 0; v < 5; ++v) P[v * n + i] = p[v];
+        if (iters) iters[i] = r;
+        if (fp64) fp64[i] = f64;
+    }
+}
+
+cudaError_t launch_point_c2p_gated(double g, const double* U, const float* W0, double rtol, int max_newton,
+                                   int max_bracket, double* P, int* iters, int* fp64, int n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_point_c2p_gated<<<grid_for(n, 128), 128, 0, s>>>(g, U, W0, rtol, max_newton, max_bracket, P, iters, fp64, n);
+    return cudaGetLastError();
+}
+
 int max_speed_blocks(const Grid& g) {
     (void)g;
     return 148 * 4;

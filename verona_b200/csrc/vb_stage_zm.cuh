@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
     const long long tot = (long long)N0 * N1 * N2;  // < 2^32 (launch_c2p)
     CellMap cm;
     cm.init(N0, N1, p.sy, p.sz, NG);
-    unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
+    unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0, n_64 = 0;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
          e += (long long)gridDim.x * blockDim.x) {
         const long long c = cm.padded((uint32_t)e);
@@ -357,12 +357,13 @@ __global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
             U[v] = b.Uo[v * p.vs + c];
             P[v] = need_p ? (double)b.Pin[v * p.vs + c] : 0.0;
         }
-        int fb;
-        int r = solve_cell<3>(p, U, P, c, fb);
+        int fb, f64 = 1;
+        int r = solve_cell<3>(p, U, P, c, fb, &f64);
         n_fail += (r < 0);
         n_fb += fb;
         n_it += (r < 0 ? -r : r);
         n_cells += 1;
+        n_64 += f64;
         P[0] = jmax(P[0], p.floor_);
         P[1] = jmax(P[1], p.floor_);
 #pragma unroll
@@ -374,11 +375,13 @@ __global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
             n_fb += __shfl_xor_sync(0xffffffffu, n_fb, o);
             n_it += __shfl_xor_sync(0xffffffffu, n_it, o);
             n_cells += __shfl_xor_sync(0xffffffffu, n_cells, o);
+            n_64 += __shfl_xor_sync(0xffffffffu, n_64, o);
         }
         if ((threadIdx.x & 31) == 0) {
             count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
             count_add(p.counters, CNT_C2P_ITERS, n_it);
             count_add(p.counters, CNT_C2P_CELLS, n_cells);
+            count_add(p.counters, CNT_C2P_FP64, n_64);
         }
     } else if (n_fb) {
         count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
@@ -441,7 +444,7 @@ template <typename R> int stage_split_c2p(int dims, const StageParams& p) {
 template <typename R>
 cudaError_t dispatch_stage_zm(int rec, int rs, const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
     if constexpr (std::is_same<R, float>::value) {
-        if (p.pairs && zp_available(rec, rs)) return launch_stage_zp(rs, p, b, s);
+        if (p.pairs && zp_available(rec, rs)) return launch_stage_zp(rec, rs, p, b, s);
     }
 #define VB_CASE(RC, RSC) \
     if (rec == RC && rs == RSC) return launch_stage_zm<RC, RSC, R>(p, b, s);

@@ -132,6 +132,20 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
     }
 }
 
+// Reconstruction of two cells: WENOZ on the packed pairs; PPM and MINMOD
+// (src/fluxlimiter.jl:1-13, 74-180) are branch-heavy limiters and run lane by
+// lane through the scalar FP32 forms of vb_physics.cuh, bit-identical to the
+// one-cell-per-thread kernel's reconstructions.
+template <int REC>
+__device__ __forceinline__ void recon2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& qr, f2& ql) {
+    if constexpr (REC == REC_WENOZ) {
+        wenoz(qm2, qm1, q0, qp1, qp2, qr, ql);
+    } else {
+        recon<REC, float>(qm2.x, qm1.x, q0.x, qp1.x, qp2.x, qr.x, ql.x);
+        recon<REC, float>(qm2.y, qm1.y, q0.y, qp1.y, qp2.y, qr.y, ql.y);
+    }
+}
+
 // One face state along axis D (compile time): the primitive state and what
 // the HARM speeds / HLL / HLLC need from it (src/3dim/algos.jl:117-157).
 // Sign convention of the energy slot: E = -U[1] > 0 and FE = -F[1].
@@ -283,7 +297,7 @@ enum { ZP_FUSED = 0, ZP_U = 1, ZP_DIV = 2 };
 // the tensor map of Pin, dims (x, y, z, variable)); otherwise the column's
 // z-window is loaded by the thread and the x/y halo of the planes (k, k+1)
 // by 4-byte asynchronous copies into an interleaved pair buffer.
-template <int RS, int TX, int TY, int LZ, int MINB, int TAIL, bool TMA>
+template <int REC, int RS, int TX, int TY, int LZ, int MINB, int TAIL, bool TMA>
 __global__ void __launch_bounds__(TX * TY, MINB)
     k_stage_zp(StageParams p, StageBufs<float> b, const __grid_constant__ CUtensorMap tm) {
     using namespace pk;
@@ -344,7 +358,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
         for (int v = 0; v < NV; ++v) {
             const float s0 = zs(c - 2, v), s1 = zs(c - 1, v), s2 = zs(c, v), s3 = zs(c + 1, v), s4 = zs(c + 2, v),
                         s5 = zs(c + 3, v);
-            wenoz(P2(s0, s1), P2(s1, s2), P2(s2, s3), P2(s3, s4), P2(s4, s5), qr[v], ql[v]);
+            recon2<REC>(P2(s0, s1), P2(s1, s2), P2(s2, s3), P2(s3, s4), P2(s4, s5), qr[v], ql[v]);
             if (v < 2) {
                 qr[v] = vmax(fl, qr[v]);
                 ql[v] = vmax(fl, ql[v]);
@@ -470,7 +484,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 f2 qr, ql;
-                wenoz(pq(v, o - 2), pq(v, o - 1), pq(v, o), pq(v, o + 1), pq(v, o + 2), qr, ql);
+                recon2<REC>(pq(v, o - 2), pq(v, o - 1), pq(v, o), pq(v, o + 1), pq(v, o + 2), qr, ql);
                 if (v < 2) {
                     qr = vmax(fl, qr);
                     ql = vmax(fl, ql);
@@ -489,7 +503,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
                 const int v = e % NV, cell = e / NV, r = cell >> 1, side = cell & 1;
                 const int o = (r + 3) * ROW + (side ? TX : -1) + 3;
                 f2 qr, ql;
-                wenoz(pq(v, o - 2), pq(v, o - 1), pq(v, o), pq(v, o + 1), pq(v, o + 2), qr, ql);
+                recon2<REC>(pq(v, o - 2), pq(v, o - 1), pq(v, o), pq(v, o + 1), pq(v, o + 2), qr, ql);
                 if (v < 2) {
                     qr = vmax(fl, qr);
                     ql = vmax(fl, ql);
@@ -532,7 +546,8 @@ __global__ void __launch_bounds__(TX * TY, MINB)
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 f2 qr, ql;
-                wenoz(pq(v, o - 2 * ROW), pq(v, o - ROW), pq(v, o), pq(v, o + ROW), pq(v, o + 2 * ROW), qr, ql);
+                recon2<REC>(pq(v, o - 2 * ROW), pq(v, o - ROW), pq(v, o), pq(v, o + ROW), pq(v, o + 2 * ROW), qr,
+                            ql);
                 if (v < 2) {
                     qr = vmax(fl, qr);
                     ql = vmax(fl, ql);
@@ -546,7 +561,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
             const int v = e / (2 * TX), cell = e % (2 * TX), cx_ = cell % TX, side = cell / TX;
             const int o = ((side ? TY : -1) + 3) * ROW + cx_ + 3;
             f2 qr, ql;
-            wenoz(pq(v, o - 2 * ROW), pq(v, o - ROW), pq(v, o), pq(v, o + ROW), pq(v, o + 2 * ROW), qr, ql);
+            recon2<REC>(pq(v, o - 2 * ROW), pq(v, o - ROW), pq(v, o), pq(v, o + ROW), pq(v, o + 2 * ROW), qr, ql);
             if (v < 2) {
                 qr = vmax(fl, qr);
                 ql = vmax(fl, ql);
@@ -699,10 +714,10 @@ struct ZpCfg {
     static constexpr int TX = 32, TY = 8, LZ = 64, MINB = 2, MINB_SPLIT = 2;
 };
 
-template <int RS, int TAIL, bool TMA>
+template <int REC, int RS, int TAIL, bool TMA>
 cudaError_t launch_stage_zp_t(const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
     using C = ZpCfg;
-    auto kern = k_stage_zp<RS, C::TX, C::TY, C::LZ, TAIL == ZP_FUSED ? C::MINB : C::MINB_SPLIT, TAIL, TMA>;
+    auto kern = k_stage_zp<REC, RS, C::TX, C::TY, C::LZ, TAIL == ZP_FUSED ? C::MINB : C::MINB_SPLIT, TAIL, TMA>;
     constexpr size_t smem = TMA ? ZpTmaGeom<C::TX, C::TY>::smem_bytes() : ZpGeom<C::TX, C::TY>::smem_bytes();
     static unsigned long long attr_set = 0;
     int dev = 0;
@@ -729,23 +744,29 @@ cudaError_t launch_stage_zp_t(const StageParams& p, const StageBufs<float>& b, c
     return cudaGetLastError();
 }
 
-// WENOZ with HLL or HLLC in the FP32-bulk form (zp_available). The divergence
-// hand-off (ZP_DIV) is taken when the caller's con2prim kernel forms U itself
-// (p.want_div, the fused learned kernel), which saves the stencil kernel every
-// FP64 load and store; the reference con2prim cascade of k_c2p, bound by its
-// own memory latency, keeps reading a formed U (ZP_U).
-template <int RS, bool TMA>
+// Every reconstruction with HLL or HLLC in the FP32-bulk form (zp_available).
+// The divergence hand-off (ZP_DIV) is taken when the caller's con2prim kernel
+// forms U itself (p.want_div, the fused learned con2prim).
+template <int REC, int RS, bool TMA>
 cudaError_t dispatch_stage_zp_tail(const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
-    if (!(p.split || p.skip_c2p)) return launch_stage_zp_t<RS, ZP_FUSED, TMA>(p, b, s);
-    if (p.skip_c2p && p.want_div) return launch_stage_zp_t<RS, ZP_DIV, TMA>(p, b, s);
-    return launch_stage_zp_t<RS, ZP_U, TMA>(p, b, s);
+    if (!(p.split || p.skip_c2p)) return launch_stage_zp_t<REC, RS, ZP_FUSED, TMA>(p, b, s);
+    if (p.skip_c2p && p.want_div) return launch_stage_zp_t<REC, RS, ZP_DIV, TMA>(p, b, s);
+    return launch_stage_zp_t<REC, RS, ZP_U, TMA>(p, b, s);
 }
 // the TMA form where the caller encoded a tensor map of Pin (p.tmap_in)
-template <int RS> cudaError_t dispatch_stage_zp_rs(const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
-    return p.tmap_in ? dispatch_stage_zp_tail<RS, true>(p, b, s) : dispatch_stage_zp_tail<RS, false>(p, b, s);
+template <int REC, int RS>
+cudaError_t dispatch_stage_zp_rs(const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
+    return p.tmap_in ? dispatch_stage_zp_tail<REC, RS, true>(p, b, s) : dispatch_stage_zp_tail<REC, RS, false>(p, b, s);
 }
-inline cudaError_t dispatch_stage_zp(int rs, const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
-    return rs == RS_HLLC ? dispatch_stage_zp_rs<RS_HLLC>(p, b, s) : dispatch_stage_zp_rs<RS_HLL>(p, b, s);
+template <int REC>
+cudaError_t dispatch_stage_zp_rec(int rs, const StageParams& p, const StageBufs<float>& b, cudaStream_t s) {
+    return rs == RS_HLLC ? dispatch_stage_zp_rs<REC, RS_HLLC>(p, b, s) : dispatch_stage_zp_rs<REC, RS_HLL>(p, b, s);
+}
+inline cudaError_t dispatch_stage_zp(int rec, int rs, const StageParams& p, const StageBufs<float>& b,
+                                     cudaStream_t s) {
+    if (rec == REC_MINMOD) return dispatch_stage_zp_rec<REC_MINMOD>(rs, p, b, s);
+    if (rec == REC_PPM) return dispatch_stage_zp_rec<REC_PPM>(rs, p, b, s);
+    return dispatch_stage_zp_rec<REC_WENOZ>(rs, p, b, s);
 }
 
 }  // namespace vb

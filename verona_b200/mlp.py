@@ -45,6 +45,7 @@ def _sig():
         "vb_mlp_get_grad": [vp, fp, vp],
         "vb_attach_mlp": [vp, vp],
         "vb_point_c2p_w": [C.c_double, vp, vp, C.c_double, C.c_int, C.c_int, vp, vp, vp, C.c_int, vp],
+        "vb_point_c2p_gated": [C.c_double, vp, vp, C.c_double, C.c_int, C.c_int, vp, vp, vp, C.c_int, vp],
     }
     for k, a in sigs.items():
         f = getattr(lib, k)
@@ -340,6 +341,21 @@ def c2p_w(U, W0, gamma, rtol=1e-12, max_newton=8, max_bracket=200):
     _chk(lib.vb_point_c2p_w(gamma, _ptr(U.contiguous()), _ptr(W0.contiguous()), rtol, max_newton, max_bracket, _ptr(P),
                             _ptr(it), _ptr(fb), n, None))
     return P, it, fb
+
+
+def c2p_gated(U, W0, gamma, rtol=1e-12, max_newton=8, max_bracket=200):
+    """vb_point_c2p_gated on (5, n) FP64 / (n,) FP32 CUDA tensors -> (P, iterations, fp64 flag)."""
+    import torch
+
+    lib = _sig()
+    n = U.shape[1]
+    P = torch.empty_like(U)
+    it = torch.empty(n, dtype=torch.int32, device="cuda")
+    f64 = torch.empty(n, dtype=torch.int32, device="cuda")
+    W0 = W0.to(torch.float32).contiguous()
+    _chk(lib.vb_point_c2p_gated(gamma, _ptr(U.contiguous()), _ptr(W0), rtol, max_newton, max_bracket, _ptr(P),
+                                _ptr(it), _ptr(f64), n, None))
+    return P, it, f64
 
 
 _cached = {}
