@@ -105,12 +105,12 @@ def device_ic(n, seed):
     return P
 
 
-def make_solver(n, precision, guess, stats=0):
+def make_solver(n, precision, guess, stats=0, c2p_fp32=0):
     from verona_b200 import Solver
 
     dx = 1.0 / n
     s = Solver(3, (n, n, n), GAMMA, (dx, dx, dx), recon="wenoz", riemann="hllc", rk=3, precision=precision,
-               guess=guess, n_iter=50, tol=1e-12, floor=1e-8, stats=stats)
+               guess=guess, n_iter=50, tol=1e-12, floor=1e-8, stats=stats, c2p_fp32=c2p_fp32)
     s.set_boundary(0, 2, nozzle(n))
     return s
 
@@ -193,14 +193,19 @@ def timed_steps(s, dt, warmup, steps, dist=None):
     return ms, stage_ms, stage_launches, launches
 
 
-def guess_comparison(n, P0, dt, W, K, dist, learned, stencil_ms_learned, stage_ms_learned, ms_learned):
+def guess_comparison(n, P0, dt, W, K, dist, learned, stencil_ms_learned, stage_ms_learned, ms_learned, P64=None,
+                     err_learned=None):
     """The learned guess against the method without it, on the same FP32-bulk
     workload, each timed like the headline (stencil and con2prim kernel timed
     apart by the library's profiling events) and run again with iteration
     statistics (W steps, counters reset, 3 steps):
-    - previous_w: the same precision-gated W Newton as the learned path,
-      warm-started from the previous state's W instead of the network (the
-      network's contribution alone);
+    - learned_gated: the learned path with the precision gate of the con2prim
+      (options.c2p_fp32: FP32 pressure Newton where the guess has Lorentz
+      factor below sqrt 2 and kinetic energy below 10 x the pressure, FP64
+      for the rest in a second pass);
+    - previous_w: the same W Newton as the learned path, warm-started from the
+      previous state's W instead of the network (the network's contribution
+      alone);
     - previous: the reference's con2prim cascade from the previous state
       (src/3dim/structs.jl:277-287); its counter records the cascade stage that
       converged (1 = the 1DW Newton), not Newton iterations."""
@@ -209,27 +214,41 @@ def guess_comparison(n, P0, dt, W, K, dist, learned, stencil_ms_learned, stage_m
     from verona_b200 import mlp
 
     out = {}
-    arms = (("learned", "learned"), ("previous_w", "previous_w"), ("previous", "previous"))
+    arms = (("learned", "learned"), ("learned_gated", "learned"), ("previous_w", "previous_w"),
+            ("previous", "previous"))
     for name, guess in arms:
-        if name == "learned" and not learned:
+        if guess == "learned" and not learned:
             continue
+        gate = int(name == "learned_gated")
         if name == "learned":
             out[name] = {"ms_per_step": ms_learned / K, "value": n**3 * K / (ms_learned / 1e3),
                          "stencil_ms_per_stage": stencil_ms_learned,
                          "c2p_ms_per_stage": stage_ms_learned - stencil_ms_learned,
+                         "l1_error_vs_fp64": err_learned,
                          "c2p_kernels": "k_c2p_learned (U from the divergence, network guess, FP32 pressure Newton) "
                                         "+ k_c2p_deferred (FP64 W Newton of the cells the gate leaves)"}
         else:
-            s = make_solver(n, "fp32", guess)
+            s = make_solver(n, "fp32", guess, c2p_fp32=gate)
+            if guess == "learned":
+                mlp.attach(s)
             s.load_prims(P0)
             ms, st_ms, st_l, _ = timed_steps(s, dt, W, K, dist)
             sten = timed_steps.stencil_ms / max(st_l, 1)
+            err = None
+            if P64 is not None:
+                Pa = s.store_prims()
+                torch.cuda.synchronize()
+                err = l1_errors(Pa, P64)
+                del Pa
             s.close()
+            kern = {"learned_gated": "k_c2p_learned with the precision gate (FP32 pressure Newton) + k_c2p_deferred "
+                                     "(FP64 W Newton of the cells the gate leaves)",
+                    "previous_w": "k_c2p (the W Newton from the previous state's W)",
+                    "previous": "k_c2p (the reference cascade from the previous primitive state)"}[name]
             out[name] = {"ms_per_step": ms / K, "value": n**3 * K / (ms / 1e3), "stencil_ms_per_stage": sten,
-                         "c2p_ms_per_stage": st_ms / max(st_l, 1) - sten,
-                         "c2p_kernels": "k_c2p (gated W Newton from the previous state's W)" if name == "previous_w"
-                         else "k_c2p (the reference cascade from the previous primitive state)"}
-        s = make_solver(n, "fp32", guess, stats=1)
+                         "c2p_ms_per_stage": st_ms / max(st_l, 1) - sten, "l1_error_vs_fp64": err,
+                         "c2p_kernels": kern}
+        s = make_solver(n, "fp32", guess, stats=1, c2p_fp32=gate)
         if guess == "learned":
             mlp.attach(s)
         s.load_prims(P0)
@@ -248,7 +267,7 @@ def guess_comparison(n, P0, dt, W, K, dist, learned, stencil_ms_learned, stage_m
             stat["newton_iters_per_cell"] = float(c[2]) / cells
         out[name].update(stat)
     if learned:
-        for base in ("previous_w", "previous"):
+        for base in ("learned_gated", "previous_w", "previous"):
             out[f"step_speedup_learned_vs_{base}"] = out[base]["ms_per_step"] / out["learned"]["ms_per_step"]
             out[f"c2p_speedup_learned_vs_{base}"] = out[base]["c2p_ms_per_stage"] / out["learned"]["c2p_ms_per_stage"]
     return out
@@ -534,11 +553,12 @@ def run_ours(args, rank, world, dist):
     info["fast_counters"] = s.counters().tolist()
     err = l1_errors(Pf, P64) if fp64 else None
     del Pf
-    if fp64:
-        del P64
     guesses = None
     if args.path == "both" and not args.no_guess_compare:
-        guesses = guess_comparison(n, P0, dt, W, K, dist, learned_ok, stencil_ms, st_ms / max(st_l, 1), ms)
+        guesses = guess_comparison(n, P0, dt, W, K, dist, learned_ok, stencil_ms, st_ms / max(st_l, 1), ms,
+                                   P64=P64 if fp64 else None, err_learned=err)
+    if fp64:
+        del P64
 
     t_tensor = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist is not None:

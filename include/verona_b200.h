@@ -96,10 +96,13 @@ typedef struct vb_options {
     double floor_;        /* density / internal-energy floor: HARM_HLL `floor` */
     double w_rtol;        /* learned guess: relative W tolerance of the refinement (1e-12) */
     int32_t w_max_newton; /* learned guess: Newton steps before the bracketed fallback (8) */
-    int32_t c2p_fp32;     /* W-Newton guesses + FP32 bulk: 1 = precision-gated con2prim (default): an
-                           * FP32 Newton on the pressure where the guess has Lorentz factor below
+    int32_t c2p_fp32;     /* W-Newton guesses + FP32 bulk: 1 = precision-gated con2prim: an FP32
+                           * Newton on the pressure where the guess has Lorentz factor below
                            * sqrt 2 and kinetic energy below 10 x the pressure, the FP64 W Newton
-                           * elsewhere; 0 = the FP64 W Newton on every cell */
+                           * elsewhere (for the learned guess, in a second kernel over the cells
+                           * the gate leaves); 0 = the FP64 W Newton on every cell (default: on
+                           * B200, whose FP64 rate is half its FP32 rate, the gate saves no time
+                           * in the latency-bound learned kernel, and the second pass costs some) */
     int32_t reserved_i[6];
     double reserved_d[4];
 } vb_options;
@@ -108,7 +111,7 @@ typedef struct vb_solver* vb_handle;
 
 /* Fill *o with the reference's defaults (WENOZ, HLL, RK2, FP64, previous-state
  * guess, n_iter 50, tol 1e-10, floor 1e-7) and the extensions' (w_rtol 1e-12,
- * w_max_newton 8, c2p_fp32 1). */
+ * w_max_newton 8, c2p_fp32 0). */
 int vb_default_options(vb_options* o);
 
 /* Create a solver for an nx x ny x nz interior grid (ny = nz = 1 in 1D,

@@ -149,16 +149,18 @@ def test_learned_solver_matches_fp64_path(net):
     assert max(per_field_rel(out["learned"][0], out["previous"][0])) < 1e-8
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_learned_fused_kernel_matches_two_kernel_form(net, precision):
+@pytest.mark.parametrize("precision,gate", [("fp64", 0), ("fp32", 0), ("fp32", 1)])
+def test_learned_fused_kernel_matches_two_kernel_form(net, precision, gate):
     """The one-kernel learned con2prim (guess + W Newton per 128-cell tile)
     against the guess kernel + con2prim kernel pair: both start each cell's
     Newton from the same FP32-rounded network guess, so they agree to the
     Newton tolerance (the two forms are built in different compilation units,
-    whose FP64 contraction may differ in the last bit). Both run the
-    one-cell-per-thread FP32 stencil kernel here; the z-pair stencil, which
-    leaves the divergence for the fused kernel to combine, is compared with it
-    at FP32 rounding."""
+    whose FP64 contraction may differ in the last bit). With the precision
+    gate (options.c2p_fp32) the fused form solves the admitted cells in FP32
+    and the rest in its FP64 pass over the list, the two-kernel form both in
+    one kernel; every cell is counted once. Both run the one-cell-per-thread
+    FP32 stencil kernel here; the z-pair stencil, which leaves the divergence
+    for the fused kernel to combine, is compared with it at FP32 rounding."""
     from helpers import jet_ic, nozzle_params, per_field_rel
     from verona_b200 import Solver
 
@@ -169,7 +171,7 @@ def test_learned_fused_kernel_matches_two_kernel_form(net, precision):
     out = {}
     for fused, pairs in ((0, 0), (1, 0), (1, 1)):
         s = Solver(3, n, G, dxs, recon="wenoz", riemann="hllc", rk=3, guess="learned", precision=precision,
-                   n_iter=50, tol=1e-12, floor=1e-8, stats=1)
+                   n_iter=50, tol=1e-12, floor=1e-8, stats=1, c2p_fp32=gate)
         net.attach(s)
         s.set_tuning(learned_fused=fused, fp32_pairs=pairs)
         assert s.get_tuning()["learned_fused"] == fused
@@ -178,8 +180,10 @@ def test_learned_fused_kernel_matches_two_kernel_form(net, precision):
         s.step(dt, 5)
         out[fused + pairs] = (s.prims(), s.cons(), s.counters())
     c0, c1 = out[0][2], out[1][2]
-    print(precision, "two-kernel counters", c0.tolist(), "fused", c1.tolist())
-    assert c1[0] == 0 and c1[4] == 0 and c1[3] == c0[3]
+    print(precision, gate, "two-kernel counters", c0.tolist(), "fused", c1.tolist())
+    assert c1[0] == 0 and c1[4] == 0 and c1[3] == c0[3] and c1[6] == c0[6]
+    if gate:
+        assert 0 < c1[6] < c1[3]  # both paths of the gate ran
     assert abs(int(c1[2]) - int(c0[2])) <= 0.01 * int(c0[2])
     ep = max(per_field_rel(out[1][0], out[0][0]))
     eu = max(per_field_rel(out[1][1], out[0][1]))
@@ -334,11 +338,12 @@ def test_learned_guess_against_the_previous_state_at_fresh_shocks(net):
 
 def test_three_guesses_in_a_jet_agree():
     """The 3D jet (WENOZ + HLLC, SSP-RK3, FP32 bulk) with the three con2prim
-    guesses -- the learned network, the previous state's W (the same gated W
-    Newton without the network), the reference cascade from the previous
-    state -- each within the FP32-bulk error bar (L1 rho 1e-5) of the FP64
-    run, without failures; the two W-Newton guesses report their Newton
-    iterations and FP64 cell counts (options.stats)."""
+    guesses -- the learned network, the previous state's W (the same W Newton
+    without the network), the reference cascade from the previous state --
+    the W-Newton guesses with and without the precision gate
+    (options.c2p_fp32), each within the FP32-bulk error bar (L1 rho 1e-5) of
+    the FP64 run, without failures; they report their Newton iterations and
+    FP64 cell fractions (options.stats)."""
     from helpers import jet_ic, nozzle_params
     from verona_b200 import Solver, mlp
 
@@ -349,21 +354,24 @@ def test_three_guesses_in_a_jet_agree():
     dt = 0.4 / sum(1.0 / d for d in dxs)
     noz = nozzle_params(3, n, 4.0, gamma=g)
     out, stats = {}, {}
-    for guess, prec in (("previous", "fp64"), ("learned", "fp32"), ("previous_w", "fp32"), ("previous", "fp32")):
+    for guess, prec, gate in (("previous", "fp64", 0), ("learned", "fp32", 0), ("learned", "fp32", 1),
+                              ("previous_w", "fp32", 0), ("previous_w", "fp32", 1), ("previous", "fp32", 0)):
         s = Solver(3, n, g, dxs, recon="wenoz", riemann="hllc", rk=3, precision=prec, guess=guess, n_iter=50,
-                   tol=1e-12, floor=1e-8, stats=1)
+                   tol=1e-12, floor=1e-8, stats=1, c2p_fp32=gate)
         if guess == "learned":
             mlp.attach(s)
         s.set_boundary(0, 2, noz)
         s.load_prims(P0)
         s.step(dt, 10)
         c = s.counters()
-        assert c[0] == 0 and c[4] == 0, (guess, prec, c)
-        out[(guess, prec)] = s.prims()[:, 3:-3, 3:-3, 3:-3]
-        stats[(guess, prec)] = (float(c[2]) / max(int(c[3]), 1), float(c[6]) / max(int(c[3]), 1))
+        assert c[0] == 0 and c[4] == 0, (guess, prec, gate, c)
+        out[(guess, prec, gate)] = s.prims()[:, 3:-3, 3:-3, 3:-3]
+        stats[(guess, prec, gate)] = (float(c[2]) / max(int(c[3]), 1), float(c[6]) / max(int(c[3]), 1))
         s.close()
-    ref = out[("previous", "fp64")]
-    for key in (("learned", "fp32"), ("previous_w", "fp32"), ("previous", "fp32")):
+    ref = out[("previous", "fp64", 0)]
+    for key in out:
+        if key == ("previous", "fp64", 0):
+            continue
         a = out[key]
         l1 = float(np.mean(np.abs(a[0] - ref[0])) / np.mean(np.abs(ref[0])))
         print(key, "L1 rho vs FP64 %.2e; iterations (stage for the cascade) %.3f, FP64 cell fraction %.4f"
