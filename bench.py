@@ -54,6 +54,8 @@ def parse():
                     help="steps of the 2D jet (config 2: 200)")
     ap.add_argument("--path", default="both", choices=["both", "fast", "fp64"],
                     help="fp64: time only the plain FP64 path (profiling runs)")
+    ap.add_argument("--fp64-contract", type=int, default=0, choices=[0, 1],
+                    help="with --path fp64: the FMA-contracted FP64 kernels (vb_tuning.fp64_contract)")
     ap.add_argument("--guess", default="auto", choices=["auto", "learned", "previous"],
                     help="con2prim guess of the fast path (auto: learned when the network is available)")
     ap.add_argument("--learned-form", default="fused", choices=["fused", "two"],
@@ -92,15 +94,18 @@ def nozzle(n):
     return [16.0, n / 2, n / 2, 0.01, 1e-3 / (GAMMA - 1), math.sqrt(99.0), 0.0, 0.0]
 
 
-def device_ic(n, seed):
-    """Primitive AoS array of the workload on the device (torch, reversed shape)."""
+def device_ic(n, seed, noise=0.03):
+    """Primitive AoS array of the workload on the device (torch, reversed shape):
+    ambient rho = 1 with `noise` relative seeded density noise, p = 1e-3, v = 0."""
     import torch
 
     m = n + 6
     gen = torch.Generator(device="cuda")
     gen.manual_seed(seed)
     P = torch.zeros((m, m, m, 5), dtype=torch.float64, device="cuda")
-    P[..., 0] = 1.0 + 0.03 * torch.randn((m, m, m), generator=gen, dtype=torch.float64, device="cuda")
+    P[..., 0] = 1.0
+    if noise:
+        P[..., 0] += noise * torch.randn((m, m, m), generator=gen, dtype=torch.float64, device="cuda")
     P[..., 1] = 1e-3 / (GAMMA - 1)
     return P
 
@@ -225,8 +230,8 @@ def guess_comparison(n, P0, dt, W, K, dist, learned, stencil_ms_learned, stage_m
                          "stencil_ms_per_stage": stencil_ms_learned,
                          "c2p_ms_per_stage": stage_ms_learned - stencil_ms_learned,
                          "l1_error_vs_fp64": err_learned,
-                         "c2p_kernels": "k_c2p_learned (U from the divergence, network guess, FP32 pressure Newton) "
-                                        "+ k_c2p_deferred (FP64 W Newton of the cells the gate leaves)"}
+                         "c2p_kernels": "k_c2p_learned (U from the divergence, network guess, FP64 W Newton "
+                                        "on every cell)"}
         else:
             s = make_solver(n, "fp32", guess, c2p_fp32=gate)
             if guess == "learned":
@@ -485,6 +490,7 @@ def run_ours(args, rank, world, dist):
     fp64 = None
     if args.path == "fp64":
         s = make_solver(n, "fp64", "previous")
+        s.set_tuning(fp64_contract=args.fp64_contract)
         s.load_prims(P0)
         ms, st_ms, st_l, ln = timed_steps(s, dt, W, K, dist)
         print(json.dumps({"path": "fp64", "zone_updates_per_s": cells * K / (ms / 1e3), "ms_per_step": ms / K,
@@ -930,26 +936,30 @@ def config1_measure(rank):
     return out
 
 
-def config3_measure(n, K, W, rank, world, dist):
-    """Config 3's precision form on the 3D jet n^3 with PPM + HLLC (SSP-RK3,
-    gamma 4/3, nozzle radius 16 cells, Lorentz 10): the FP32-bulk form and
-    the plain FP64 path (FMA-contracted) over the same K steps after W from
-    the same state, with the L1 rho / p and max Lorentz-factor errors of the
-    FP32-bulk result against the FP64 one."""
+def config3_measure(n, K, W, rank, world, dist, recon="ppm", noise=0.03, learned=False):
+    """A precision form on the 3D jet n^3 with `recon` + HLLC (SSP-RK3, gamma
+    4/3, nozzle radius 16 cells, Lorentz 10; config 3 is PPM): the FP32-bulk
+    form (with the learned guess if `learned`) and the plain FP64 path
+    (FMA-contracted) over the same K steps after W from the same state, with
+    the L1 rho / p and max Lorentz-factor errors of the FP32-bulk result
+    against the FP64 one."""
     import torch
 
-    from verona_b200 import Solver
+    from verona_b200 import Solver, mlp
 
     dx = 1.0 / n
     dt = dt_of(n)
-    P0 = device_ic(n, 42 + rank)
+    P0 = device_ic(n, 42 + rank, noise)
     hbm_peak, hbm_kind = read_peaks()
     res, outs = {}, {}
     for prec in ("fp32", "fp64"):
-        s = Solver(3, (n, n, n), GAMMA, (dx, dx, dx), recon="ppm", riemann="hllc", rk=3, precision=prec,
-                   n_iter=50, tol=1e-12, floor=1e-8)
+        guess = "learned" if (learned and prec == "fp32") else "previous"
+        s = Solver(3, (n, n, n), GAMMA, (dx, dx, dx), recon=recon, riemann="hllc", rk=3, precision=prec,
+                   guess=guess, n_iter=50, tol=1e-12, floor=1e-8)
         s.set_tuning(fp64_contract=int(prec == "fp64"))
         s.set_boundary(0, 2, nozzle(n))
+        if guess == "learned":
+            mlp.attach(s)
         s.load_prims(P0)
         ms, st_ms, st_l, _ = timed_steps(s, dt, W, K, dist)
         v = world * n**3 * K / (ms / 1e3)
@@ -986,6 +996,12 @@ def configs_measure(args, rank, world, dist):
     torch.cuda.empty_cache()
     out["config3_3d_jet_512_ppm"] = dict(config3_measure(args.n, K, W, rank, world, dist),
                                          workload=f"3D jet {args.n}^3, PPM+HLLC, SSP-RK3, nozzle r=16 Gamma=10")
+    torch.cuda.empty_cache()
+    # the headline workload on the configured noise-free ambient
+    out["config4_noise_free"] = dict(config3_measure(args.n, K, W, rank, world, dist, recon="wenoz", noise=0.0,
+                                                     learned=True),
+                                     workload=f"3D jet {args.n}^3, WENOZ+HLLC, SSP-RK3, nozzle r=16 Gamma=10, "
+                                              "ambient rho=1 p=1e-3 without noise; fp32 = learned guess")
     torch.cuda.empty_cache()
     b = batch_measure(K, W, rank, world, dist, e2e_on=False, single_on=False)
     out["config5_batch_256"] = {k: b[k] for k in ("value", "ms_per_step", "roofline", "counters", "config")}

@@ -166,6 +166,11 @@ def test_learned_fused_kernel_matches_two_kernel_form(net, precision, gate):
 
     n = (32, 16, 24)
     P0 = jet_ic(3, n, gamma=G, noise=0.03, seed=5)
+    if gate:
+        # a slab moving at Lorentz factor 1.8 (v^2 = 0.69): cells the gate
+        # rejects from the first step on (in 5 steps the beam itself only
+        # reaches the first interior cell)
+        P0[2, :, :, : 3 + 12] = 1.5
     dxs = [1.0 / 32] * 3
     dt = 0.4 / sum(1.0 / d for d in dxs)
     out = {}

@@ -78,6 +78,8 @@ __device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 __device__ __forceinline__ f2 sel(m2 m, f2 a, f2 b) { return P2(m.x ? a.x : b.x, m.y ? a.y : b.y); }
 
+__device__ __forceinline__ f2 num_scale(f2 num, f2 den_other) { return mul(num, den_other); }
+
 // WENOZ (src/fluxlimiter.jl:19-71) on two cells: returns (qr_i, ql_ip1).
 // Written on the one-sided differences D1..D4 of the five values, which the
 // smoothness indicators and the three stencils share:
@@ -86,8 +88,11 @@ __device__ __forceinline__ f2 sel(m2 m, f2 a, f2 b) { return P2(m.x ? a.x : b.x,
 //   face value = q_i + sum_k d_k s_k g_k / sum_k d_k s_k, g_k = f_k - q_i,
 //   s_k = 1 + (tau5 / (beta_k + eps))^2, d = (0.1, 0.6, 0.3).
 // The common factor 13/12 of the betas cancels in tau5 / beta except against
-// the FP32 epsilon (1e-30, an effective 1.08e-30); the smoothness ratio is
-// capped at 1e15 as in the scalar FP32 form.
+// the FP32 epsilon (1e-30, an effective 1.08e-30). The smoothness ratio is
+// capped at 1e9, so every s_k <= 1e18 and the two faces' denominators share
+// one reciprocal of their product (<= 1e36, inside the FP32 range): at FP32
+// precision a weight ratio beyond 1e8 already acts as infinite, so the cap
+// (1e15 in the scalar FP32 form) changes no selected stencil.
 __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& qr, f2& ql) {
     const f2 D1 = sub(qm1, qm2), D2 = sub(q0, qm1), D3 = sub(qp1, q0), D4 = sub(qp2, qp1);
     const f2 r = S2(3.0f / 13.0f);
@@ -105,20 +110,20 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
     f2 i1 = mul(tau, rcp(add(b1, eps)));
     f2 i2 = mul(tau, rcp(add(b2, eps)));
     f2 i3 = mul(tau, rcp(add(b3, eps)));
-    i1 = P2(fminf(i1.x, 1.0e15f), fminf(i1.y, 1.0e15f));
-    i2 = P2(fminf(i2.x, 1.0e15f), fminf(i2.y, 1.0e15f));
-    i3 = P2(fminf(i3.x, 1.0e15f), fminf(i3.y, 1.0e15f));
+    i1 = P2(fminf(i1.x, 1.0e9f), fminf(i1.y, 1.0e9f));
+    i2 = P2(fminf(i2.x, 1.0e9f), fminf(i2.y, 1.0e9f));
+    i3 = P2(fminf(i3.x, 1.0e9f), fminf(i3.y, 1.0e9f));
     const f2 one = S2(1.0f);
     const f2 s1 = fma(i1, i1, one), s2 = fma(i2, i2, one), s3 = fma(i3, i3, one);
     // right face of cell i (left-biased stencils), weights d_k folded into g_k:
     // 0.1 g1 = 0.1 (5 D2 - 2 D1) / 6, 0.6 g2 = 0.6 (D2 + 2 D3) / 6, 0.3 g3 = 0.3 (4 D3 - D4) / 6
+    f2 numl, denl, numr, denr;
     {
         const f2 g1 = fma(S2(0.5f / 6.0f), D2, mul(S2(-0.2f / 6.0f), D1));
         const f2 g2 = fma(S2(1.2f / 6.0f), D3, mul(S2(0.6f / 6.0f), D2));
         const f2 g3 = fma(S2(1.2f / 6.0f), D3, mul(S2(-0.3f / 6.0f), D4));
-        const f2 num = fma(s3, g3, fma(s2, g2, mul(s1, g1)));
-        const f2 den = fma(S2(0.3f), s3, fma(S2(0.6f), s2, mul(S2(0.1f), s1)));
-        ql = fma(num, rcp(den), q0);
+        numl = fma(s3, g3, fma(s2, g2, mul(s1, g1)));
+        denl = fma(S2(0.3f), s3, fma(S2(0.6f), s2, mul(S2(0.1f), s1)));
     }
     // left face of cell i (right-biased stencils), d = (0.1, 0.6, 0.3) on (s3, s2, s1):
     // 0.1 (2 D4 - 5 D3) / 6, 0.6 (-D3 - 2 D2) / 6, 0.3 (D1 - 4 D2) / 6
@@ -126,10 +131,13 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
         const f2 g1 = fma(S2(0.2f / 6.0f), D4, mul(S2(-0.5f / 6.0f), D3));
         const f2 g2 = fma(S2(-1.2f / 6.0f), D2, mul(S2(-0.6f / 6.0f), D3));
         const f2 g3 = fma(S2(-1.2f / 6.0f), D2, mul(S2(0.3f / 6.0f), D1));
-        const f2 num = fma(s1, g3, fma(s2, g2, mul(s3, g1)));
-        const f2 den = fma(S2(0.3f), s1, fma(S2(0.6f), s2, mul(S2(0.1f), s3)));
-        qr = fma(num, rcp(den), q0);
+        numr = fma(s1, g3, fma(s2, g2, mul(s3, g1)));
+        denr = fma(S2(0.3f), s1, fma(S2(0.6f), s2, mul(S2(0.1f), s3)));
     }
+    // 1 / denl = denr / (denl denr), 1 / denr = denl / (denl denr): one reciprocal
+    const f2 rd = rcp(mul(denl, denr));
+    ql = fma(num_scale(numl, denr), rd, q0);
+    qr = fma(num_scale(numr, denl), rd, q0);
 }
 
 // Reconstruction of two cells: WENOZ on the packed pairs; PPM and MINMOD
@@ -161,14 +169,17 @@ template <int D> struct Side {
         const f2 un = P[2 + D];
         gw = mul(gam, w);
         uw = mul(un, w);
-        const f2 igam = rcp(gam);
-        vn = mul(un, igam);
         p = mul(gm1, P[1]);
         np = mul(S2(-1.0f), p);
         // C^2 = Gamma (Gamma - 1) u / (rho + Gamma u) = Gamma p / w  (SoundSpeed, src/eos.jl:15-21), so
-        // sig = C^2 / (gam^2 (1 - C^2)) = Gamma p / (gam^2 (w - Gamma p)), w - Gamma p > 0: one reciprocal
+        // sig = C^2 / (gam^2 (1 - C^2)) = Gamma p / (gam^2 (w - Gamma p)), w - Gamma p > 0. With
+        // R = 1 / (gam (w - Gamma p)), one reciprocal: 1 / gam = (w - Gamma p) R, sig = Gamma p R / gam
         const f2 gp = mul(g, p);
-        const f2 sig = mul(mul(gp, mul(igam, igam)), rcp(sub(w, gp)));
+        const f2 wgp = sub(w, gp);
+        const f2 R = rcp(mul(gam, wgp));
+        const f2 igam = mul(wgp, R);
+        vn = mul(un, igam);
+        const f2 sig = mul(mul(gp, R), igam);
         const f2 r = vsqrt(mul(sig, add(sub(one, mul(vn, vn)), sig)));
         const f2 inv = rcp(add(one, sig));
         lp = mul(add(vn, r), inv);
@@ -259,9 +270,10 @@ template <int TX, int TY> struct ZpGeom {
     static constexpr int FXN = (TX + 1) * TY, FYN = TX * (TY + 1);
     static constexpr int FN = FXN > FYN ? FXN : FYN;
     static constexpr int QXN = TX > TY ? TX : TY;
+    static constexpr int YHN = 2 * TX;  // y-halo states: ql of the cells of row -1, qr of row TY
     static constexpr int ZR = 6;  // z-window ring: planes k-1 .. k+4
     static constexpr size_t smem_bytes() {
-        return sizeof(float2) * NV * (size_t)(PLN + 2 * FN + QXN) + sizeof(float) * (size_t)ZR * NV * NT;
+        return sizeof(float2) * NV * (size_t)(PLN + 2 * FN + QXN + YHN) + sizeof(float) * (size_t)ZR * NV * NT;
     }
 };
 
@@ -277,7 +289,7 @@ template <int TX, int TY> struct ZpTmaGeom {
     static constexpr int SLOTF = (BOX_BYTES + 127) / 128 * 128 / 4;  // floats per slot (128-byte aligned)
     static constexpr size_t smem_bytes() {
         using G = ZpGeom<TX, TY>;
-        return 128 + 4 * (size_t)ZR * SLOTF + sizeof(float2) * NV * (size_t)(2 * G::FN + G::QXN) + 8 * ZR;
+        return 128 + 4 * (size_t)ZR * SLOTF + sizeof(float2) * NV * (size_t)(2 * G::FN + G::QXN + G::YHN) + 8 * ZR;
     }
 };
 // the TMA rules and the residency the launch bound assumes (2 CTAs per SM)
@@ -314,19 +326,22 @@ __global__ void __launch_bounds__(TX * TY, MINB)
     float* sRing = nullptr;    // TMA form: [ZR][SLOTF] plane boxes
     uint64_t* sBar = nullptr;  // TMA form: one mbarrier per ring slot
     f2 *sQL, *sF, *sQX;        // [NV][FN] left states, [NV][FN] fluxes, [NV][QXN] last right states
+    f2* sYH;                   // [NV][2 TX]: ql of the cells of row -1, qr of the cells of row TY
     if constexpr (TMA) {
         unsigned char* base = smem_raw + ((128u - (tc::smem_u32(smem_raw) & 127u)) & 127u);
         sRing = reinterpret_cast<float*>(base);
         sQL = reinterpret_cast<f2*>(sRing + ZR * SLOTF);
         sF = sQL + NV * FN;
         sQX = sF + NV * FN;
-        sBar = reinterpret_cast<uint64_t*>(sQX + NV * QXN);
+        sYH = sQX + NV * QXN;
+        sBar = reinterpret_cast<uint64_t*>(sYH + NV * G::YHN);
     } else {
         sPl = reinterpret_cast<f2*>(smem_raw);
         sQL = sPl + NV * G::PLN;
         sF = sQL + NV * FN;
         sQX = sF + NV * FN;
-        sZ = reinterpret_cast<float*>(sQX + NV * QXN);
+        sYH = sQX + NV * QXN;
+        sZ = reinterpret_cast<float*>(sYH + NV * G::YHN);
     }
 
     const int tid = threadIdx.x;
@@ -523,16 +538,37 @@ __global__ void __launch_bounds__(TX * TY, MINB)
 #pragma unroll
             for (int v = 0; v < NV; ++v) sF[v * FN + ty * FXR + tx] = F[v];
         }
-        for (int e = NT - 1 - tid; e >= 0 && e < TY; e += NT) {
-            f2 PL[NV], PR[NV], F[NV];
+        // the last warp computes the TY faces at the tiles' x edge; meanwhile the
+        // other warps reconstruct the y halo (cells -1 and TY of every column,
+        // one (cell, variable) per thread) from the planes already staged, into
+        // buffers of its own, so that the y phase below has no halo work
+        static_assert(TY <= 32 && NT > 32, "x-edge faces fit the last warp");
+        if (tid >= NT - 32) {
+            const int e = NT - 1 - tid;
+            if (e < TY) {
+                f2 PL[NV], PR[NV], F[NV];
 #pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                PL[v] = sQL[v * FN + e * FXR + TX];
-                PR[v] = sQX[v * QXN + e];
+                for (int v = 0; v < NV; ++v) {
+                    PL[v] = sQL[v * FN + e * FXR + TX];
+                    PR[v] = sQX[v * QXN + e];
+                }
+                face_flux<0, RS>(g, gm1, PL, PR, F);
+#pragma unroll
+                for (int v = 0; v < NV; ++v) sF[v * FN + e * FXR + TX] = F[v];
             }
-            face_flux<0, RS>(g, gm1, PL, PR, F);
-#pragma unroll
-            for (int v = 0; v < NV; ++v) sF[v * FN + e * FXR + TX] = F[v];
+        } else {
+            for (int e = tid; e < 2 * TX * NV; e += NT - 32) {
+                const int v = e / (2 * TX), cell = e % (2 * TX), cx_ = cell % TX, side = cell / TX;
+                const int o = ((side ? TY : -1) + 3) * ROW + cx_ + 3;
+                f2 qr, ql;
+                recon2<REC>(pq(v, o - 2 * ROW), pq(v, o - ROW), pq(v, o), pq(v, o + ROW), pq(v, o + 2 * ROW), qr,
+                            ql);
+                if (v < 2) {
+                    qr = vmax(fl, qr);
+                    ql = vmax(fl, ql);
+                }
+                sYH[v * (2 * TX) + side * TX + cx_] = side ? qr : ql;
+            }
         }
         __syncthreads();
 #pragma unroll
@@ -556,21 +592,6 @@ __global__ void __launch_bounds__(TX * TY, MINB)
                 sQL[v * FN + (ty + 1) * TX + tx] = ql;
             }
         }
-        // halo cells -1 and TY of every column, one (cell, variable) per thread
-        for (int e = tid; e < 2 * TX * NV; e += NT) {
-            const int v = e / (2 * TX), cell = e % (2 * TX), cx_ = cell % TX, side = cell / TX;
-            const int o = ((side ? TY : -1) + 3) * ROW + cx_ + 3;
-            f2 qr, ql;
-            recon2<REC>(pq(v, o - 2 * ROW), pq(v, o - ROW), pq(v, o), pq(v, o + ROW), pq(v, o + 2 * ROW), qr, ql);
-            if (v < 2) {
-                qr = vmax(fl, qr);
-                ql = vmax(fl, ql);
-            }
-            if (side)
-                sQX[v * QXN + cx_] = qr;
-            else
-                sQL[v * FN + cx_] = ql;
-        }
         __syncthreads();
         // every read of sPl for this pair is done: fetch the next pair's halo
         if constexpr (!TMA) {
@@ -579,7 +600,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
         {
             f2 PL[NV], F[NV];
 #pragma unroll
-            for (int v = 0; v < NV; ++v) PL[v] = sQL[v * FN + ty * TX + tx];
+            for (int v = 0; v < NV; ++v) PL[v] = ty == 0 ? sYH[v * (2 * TX) + tx] : sQL[v * FN + ty * TX + tx];
             face_flux<1, RS>(g, gm1, PL, qry, F);
 #pragma unroll
             for (int v = 0; v < NV; ++v) sF[v * FN + ty * TX + tx] = F[v];
@@ -589,7 +610,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 PL[v] = sQL[v * FN + TY * TX + e];
-                PR[v] = sQX[v * QXN + e];
+                PR[v] = sYH[v * (2 * TX) + TX + e];
             }
             face_flux<1, RS>(g, gm1, PL, PR, F);
 #pragma unroll

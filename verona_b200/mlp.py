@@ -304,6 +304,24 @@ class MLP:
                 log(f"epoch {ep}: mse {hist[-1]:.3e}")
         return hist
 
+    def evaluate(self, n=1 << 16, gamma=4.0 / 3.0, seed=99, lorentz_max=50.0):
+        """Held-out quality of the guess: relative W0 error (median, 99th
+        percentile) and the bracketed W Newton's mean iterations and
+        fallbacks from it, on n synthetic states that no training set draws
+        (seed 99, Lorentz factor up to lorentz_max)."""
+        P = synthetic_states(n, gamma, seed=seed, lorentz_max=lorentz_max)
+        U = prim2con_torch(P, gamma)
+        f, _ = self.features(U, None, gamma)
+        y = self.forward(f).double()
+        W0 = -U[1] * (1 + y.clamp(min=0))
+        Wt = (gamma - 1) * P[1] - U[1]
+        err = ((W0 - Wt) / Wt).abs()
+        _, it, fb = c2p_w(U, W0, gamma)
+        it = it.double()
+        return {"w0_rel_err_median": err.median().item(), "w0_rel_err_p99": err.quantile(0.99).item(),
+                "newton_iters_mean": it[it > 0].mean().item(), "fallbacks": int(fb.sum().item()),
+                "failures": int((it <= 0).sum().item()), "states": n}
+
     def save(self, path=DEFAULT_WEIGHTS):
         os.makedirs(os.path.dirname(path), exist_ok=True)
         np.savez(path, params=self.params(), norm=self.norm)
@@ -402,12 +420,20 @@ def main(argv=None):
     ap.add_argument("--samples", type=int, default=1 << 22)
     ap.add_argument("--epochs", type=int, default=4)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--evaluate", action="store_true", help="print the held-out W0 error and Newton iterations")
+    ap.add_argument("--no-save", action="store_true", help="train (and evaluate) without writing the weights")
     a = ap.parse_args(argv)
     t0 = time.time()
     m = MLP(seed=a.seed)
     hist = m.train(n_samples=a.samples, epochs=a.epochs, seed=a.seed, log=print)
-    m.save(a.out)
-    print(f"saved {a.out}: {n_params()} parameters, loss per epoch {hist}, {time.time() - t0:.1f} s")
+    t_train = time.time() - t0
+    if not a.no_save:
+        m.save(a.out)
+        print(f"saved {a.out}")
+    print(f"{n_params()} parameters, {a.samples} samples x {a.epochs} epochs, loss per epoch {hist}, "
+          f"{t_train:.1f} s")
+    if a.evaluate:
+        print("held-out:", m.evaluate())
 
 
 if __name__ == "__main__":
