@@ -21,12 +21,15 @@ VB_HD void solve3(const double* A, const double* b, double* x) {
     double c2 = a(3, 2) * a(1, 3) - a(1, 2) * a(3, 3);
     double c3 = a(1, 2) * a(2, 3) - a(2, 2) * a(1, 3);
     double det = a(1, 1) * c1 + a(2, 1) * c2 + a(3, 1) * c3;
-    x[0] = ((a(2, 2) * a(3, 3) - a(2, 3) * a(3, 2)) * b[0] + (a(1, 3) * a(3, 2) - a(1, 2) * a(3, 3)) * b[1] +
-            (a(1, 2) * a(2, 3) - a(1, 3) * a(2, 2)) * b[2]) / det;
-    x[1] = ((a(2, 3) * a(3, 1) - a(2, 1) * a(3, 3)) * b[0] + (a(1, 1) * a(3, 3) - a(1, 3) * a(3, 1)) * b[1] +
-            (a(1, 3) * a(2, 1) - a(1, 1) * a(2, 3)) * b[2]) / det;
-    x[2] = ((a(2, 1) * a(3, 2) - a(2, 2) * a(3, 1)) * b[0] + (a(1, 2) * a(3, 1) - a(1, 1) * a(3, 2)) * b[1] +
-            (a(1, 1) * a(2, 2) - a(1, 2) * a(2, 1)) * b[2]) / det;
+    x[0] = qdiv((a(2, 2) * a(3, 3) - a(2, 3) * a(3, 2)) * b[0] + (a(1, 3) * a(3, 2) - a(1, 2) * a(3, 3)) * b[1] +
+                    (a(1, 2) * a(2, 3) - a(1, 3) * a(2, 2)) * b[2],
+                det);
+    x[1] = qdiv((a(2, 3) * a(3, 1) - a(2, 1) * a(3, 3)) * b[0] + (a(1, 1) * a(3, 3) - a(1, 3) * a(3, 1)) * b[1] +
+                    (a(1, 3) * a(2, 1) - a(1, 1) * a(2, 3)) * b[2],
+                det);
+    x[2] = qdiv((a(2, 1) * a(3, 2) - a(2, 2) * a(3, 1)) * b[0] + (a(1, 2) * a(3, 1) - a(1, 1) * a(3, 2)) * b[1] +
+                    (a(1, 1) * a(2, 2) - a(1, 2) * a(2, 1)) * b[2],
+                det);
 #undef a
 }
 
@@ -46,7 +49,7 @@ VB_HD int c2p_1d(double g, int n_iter, double tol, const double* U, double* P) {
         double wj = g * x2 + x1;
         J[0] = gj;
         J[3] = 0.0;
-        J[6] = x1 * x3 / gj;
+        J[6] = qdiv(x1 * x3, gj);
         J[1] = -sq(gj);
         J[4] = (g - 1.0) - sq(gj) * g;
         J[7] = -2.0 * x3 * wj;
@@ -57,7 +60,7 @@ VB_HD int c2p_1d(double g, int n_iter, double tol, const double* U, double* P) {
         f[1] = f[1] - U[1];
         f[2] = f[2] - U[2];
         solve3(J, f, dl);
-        if (sqrt(sq(dl[0]) + sq(dl[1]) + sq(dl[2])) < tol) break;
+        if (qsqrt(sq(dl[0]) + sq(dl[1]) + sq(dl[2])) < tol) break;
         x1 = x1 - dl[0];
         x2 = x2 - dl[1];
         x3 = x3 - dl[2];
@@ -117,7 +120,7 @@ VB_HD bool lu_pivot4(double* A, double* t, double* x) {
         }
 #pragma unroll
         for (int i = k + 1; i <= 4; ++i) {
-            A[I4(i, k)] /= A[I4(k, k)];
+            A[I4(i, k)] = qdiv(A[I4(i, k)], A[I4(k, k)]);
 #pragma unroll
             for (int j = k + 1; j <= 4; ++j) A[I4(i, j)] = fma(-A[I4(i, k)], A[I4(k, j)], A[I4(i, j)]);
         }
@@ -132,7 +135,7 @@ VB_HD bool lu_pivot4(double* A, double* t, double* x) {
     for (int i = 4; i >= 1; --i) {
 #pragma unroll
         for (int j = i + 1; j <= 4; ++j) x[i - 1] = fma(-A[I4(i, j)], x[j - 1], x[i - 1]);
-        x[i - 1] /= A[I4(i, i)];
+        x[i - 1] = qdiv(x[i - 1], A[I4(i, i)]);
     }
 #undef I4
     return true;
@@ -152,8 +155,8 @@ VB_HD int c2p_2d(double g, int n_iter, double tol, const double* U, double* P) {
         f[3] = P[3] * gam * w - U[3];
         J[0] = gam;
         J[4] = 0.0;
-        J[8] = P[0] * P[2] / gam;
-        J[12] = P[0] * P[3] / gam;
+        J[8] = qdiv(P[0] * P[2], gam);
+        J[12] = qdiv(P[0] * P[3], gam);
         J[1] = -sq(gam);
         J[5] = (g - 1.0) - sq(gam) * g;
         J[9] = -2.0 * P[2] * w;
@@ -161,13 +164,13 @@ VB_HD int c2p_2d(double g, int n_iter, double tol, const double* U, double* P) {
         J[2] = gam * P[2];
         J[6] = gam * P[2] * g;
         J[10] = (2.0 * sq(P[2]) + sq(P[3]) + 1.0) / gam * w;
-        J[14] = P[2] * P[3] / gam * w;
+        J[14] = qdiv(P[2] * P[3], gam) * w;
         J[3] = gam * P[3];
         J[7] = gam * P[3] * g;
-        J[11] = P[2] * P[3] / gam * w;
+        J[11] = qdiv(P[2] * P[3], gam) * w;
         J[15] = (2.0 * sq(P[3]) + sq(P[2]) + 1.0) / gam * w;
         if (!lu_pivot4(J, f, o)) return -1;
-        if (sqrt(sq(o[0]) + sq(o[1]) + sq(o[2]) + sq(o[3])) < tol) break;
+        if (qsqrt(sq(o[0]) + sq(o[1]) + sq(o[2]) + sq(o[3])) < tol) break;
         P[0] = P[0] - o[0];
         P[1] = P[1] - o[1];
         P[2] = P[2] - o[2];
@@ -181,7 +184,7 @@ template <int N> VB_HD void lu_plain(double* A, const double* t, double* x) {
 #define IX(i, j) (((j)-1) * N + (i)-1)
     for (int k = 1; k <= N; ++k)
         for (int i = k + 1; i <= N; ++i) {
-            A[IX(i, k)] /= A[IX(k, k)];
+            A[IX(i, k)] = qdiv(A[IX(i, k)], A[IX(k, k)]);
             for (int j = k + 1; j <= N; ++j) A[IX(i, j)] -= A[IX(i, k)] * A[IX(k, j)];
         }
     for (int i = 1; i <= N; ++i) {
@@ -190,7 +193,7 @@ template <int N> VB_HD void lu_plain(double* A, const double* t, double* x) {
     }
     for (int i = N; i >= 1; --i) {
         for (int j = i + 1; j <= N; ++j) x[i - 1] -= A[IX(i, j)] * x[j - 1];
-        x[i - 1] /= A[IX(i, i)];
+        x[i - 1] = qdiv(x[i - 1], A[IX(i, i)]);
     }
 #undef IX
 }
@@ -198,16 +201,16 @@ template <int N> VB_HD void lu_plain(double* A, const double* t, double* x) {
 // Final primitive state from a converged W (src/3dim/structs.jl:598-609).
 VB_HD void prims_from_W(double g, double D, double Qx, double Qy, double Qz, double S2, double W,
                         double* P) {
-    double v2 = S2 / sq(W);
+    double v2 = qdiv(S2, sq(W));
     double gm = 1.0 / sqrt(1.0 - v2);
     gm = jmin(gm, 50.0);
     double rho = jmax(1e-8, D / gm);
     double UU = jmax(1e-8, (W / sq(gm) - D / gm) / g);
     P[0] = rho;
     P[1] = UU;
-    P[2] = gm * Qx / W;
-    P[3] = gm * Qy / W;
-    P[4] = gm * Qz / W;
+    P[2] = qdiv(gm * Qx, W);
+    P[3] = qdiv(gm * Qy, W);
+    P[4] = qdiv(gm * Qz, W);
 }
 
 #ifdef __CUDA_ARCH__
@@ -233,12 +236,12 @@ VB_HD int c2p_3d(double g, int n_iter, double tol, const double* Uc, double* P) 
         double w_small = P[0] + g * P[1];
         W = w_small * sq(gm);
         const double W_max = 1e30;
-        double W_min = sqrt(S2) * (1.0 + 1e-15);
-        for (int guard = 0; guard < 400 && S2 / sq(W) >= 1.0 && W < W_max; ++guard) W *= 10.0;
-        v2 = jmin(S2 / sq(W), 1.0 - 1e-15);
+        double W_min = qsqrt(S2) * (1.0 + 1e-15);
+        for (int guard = 0; guard < 400 && qdiv(S2, sq(W)) >= 1.0 && W < W_max; ++guard) W *= 10.0;
+        v2 = jmin(qdiv(S2, sq(W)), 1.0 - 1e-15);
         for (int it = 0; it < n_iter; ++it) {
             if (W < W_min) W = W_min;
-            v2 = S2 / sq(W);
+            v2 = qdiv(S2, sq(W));
             if (v2 < 0.0)
                 v2 = 0.0;
             else if (v2 > 1.0 - 1e-15)
@@ -247,8 +250,8 @@ VB_HD int c2p_3d(double g, int n_iter, double tol, const double* Uc, double* P) 
             double bf = Q_t + W - k * (W * (1.0 - v2) - D * sqrt(1.0 - v2));
             double W3 = W * W * W;
             double bj = 1.0 - ((g - 1.0) / g) * (1.0 - v2) -
-                        ((g - 1.0) / g) * (W * (2.0 * S2 / W3) - D * (S2 / (W3 * sqrt(1.0 - v2))));
-            double dW = bf / bj;
+                        ((g - 1.0) / g) * (W * qdiv(2.0 * S2, W3) - D * qdiv(S2, W3 * sqrt(1.0 - v2)));
+            double dW = qdiv(bf, bj);
             double Wp = W - dW;
             if (Wp < W_min)
                 W = 0.5 * (W + W_min);
@@ -519,7 +522,7 @@ VB_HD int c2p_w(double g, const double* Uc, double W0, double rtol, int max_newt
     const double D = Uc[0], Q_t = Uc[1];
     const double Qx = Uc[2], Qy = Uc[3], Qz = Uc[4];
     const double S2 = Qx * Qx + Qy * Qy + Qz * Qz;
-    const double Wlo0 = sqrt(S2) * (1.0 + 1e-15);
+    const double Wlo0 = qsqrt(S2) * (1.0 + 1e-15);
     const double k = (g - 1.0) / g;
     double W = W0;
     int it = 0;

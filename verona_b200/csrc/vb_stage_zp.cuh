@@ -140,14 +140,90 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
     qr = fma(num_scale(numr, denl), rd, q0);
 }
 
-// Reconstruction of two cells: WENOZ on the packed pairs; PPM and MINMOD
-// (src/fluxlimiter.jl:1-13, 74-180) are branch-heavy limiters and run lane by
-// lane through the scalar FP32 forms of vb_physics.cuh, bit-identical to the
-// one-cell-per-thread kernel's reconstructions.
+// Monotonicity limit of PPM on one lane: the reference's
+// sign(a) == sign(b) == sign(c) ? sign(a) min(C2 |b|, C2 |c|, |a|) : 0, with
+// C2 |b| and C2 |c| already formed (a zero or NaN a gives 0, as there).
+__device__ __forceinline__ float ppm_mc(float a, float b, float c, float cb, float cc) {
+    const bool same = (a > 0.0f && b > 0.0f && c > 0.0f) || (a < 0.0f && b < 0.0f && c < 0.0f);
+    return same ? copysignf(minn(cb, minn(cc, fabsf(a))), a) : 0.0f;
+}
+
+// PPM (src/fluxlimiter.jl:74-180) on two cells: the interface values, their
+// limiting and the parabola's monotonicity fix as packed arithmetic, the
+// sign tests, minima and the final choices per lane as selects (the scalar
+// form branches on every one of them). Arithmetic differs from the scalar
+// FP32 limiter in rounding only: 1/6 and 0.5 folded into fma, the ratio
+// qe / d2qf from the approximate reciprocal.
+__device__ __forceinline__ void ppm2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& qr, f2& ql) {
+    const f2 h = S2(0.5f), c2 = S2(1.25f), mtwo = S2(-2.0f);
+    const f2 qa = sub(q0, qm1), qb = sub(qp1, q0);
+    const f2 sm = add(qm1, q0), sp = add(q0, qp1);
+    // dd_im1 - dd = 0.5 (qm1 - qm2 - qb), dd - dd_ip1 = 0.5 (qa - (qp2 - qp1))
+    f2 dph = fma(h, sm, mul(S2(0.5f / 6.0f), sub(sub(qm1, qm2), qb)));
+    f2 dphp = fma(h, sp, mul(S2(0.5f / 6.0f), sub(qa, sub(qp2, qp1))));
+    const f2 d2m = fma(mtwo, qm1, add(qm2, q0));
+    const f2 d2c = fma(mtwo, q0, add(qm1, qp1));
+    const f2 d2p = fma(mtwo, qp1, add(q0, qp2));
+    const f2 cm = mul(c2, vabs(d2m)), cc = mul(c2, vabs(d2c)), cp = mul(c2, vabs(d2p));
+    {  // limit the left interface value
+        const f2 A = mul(S2(3.0f), fma(mtwo, dph, sm));
+        const f2 qd = P2(ppm_mc(A.x, d2m.x, d2c.x, cm.x, cc.x), ppm_mc(A.y, d2m.y, d2c.y, cm.y, cc.y));
+        const f2 cand = fma(S2(-1.0f / 6.0f), qd, mul(h, sm));
+        const f2 t = mul(sub(dph, qm1), sub(q0, dph));
+        dph = sel(m2{t.x < 0.0f, t.y < 0.0f}, cand, dph);
+    }
+    {  // and the right one
+        const f2 A = mul(S2(3.0f), fma(mtwo, dphp, sp));
+        const f2 qd = P2(ppm_mc(A.x, d2c.x, d2p.x, cc.x, cp.x), ppm_mc(A.y, d2c.y, d2p.y, cc.y, cp.y));
+        const f2 cand = fma(S2(-1.0f / 6.0f), qd, mul(h, sp));
+        const f2 t = mul(sub(dphp, q0), sub(qp1, dphp));
+        dphp = sel(m2{t.x < 0.0f, t.y < 0.0f}, cand, dphp);
+    }
+    const f2 d2qf = mul(S2(6.0f), fma(mtwo, q0, add(dph, dphp)));
+    const f2 dqm = sub(q0, dph), dqp = sub(dphp, q0);
+    const f2 at = mul(dqm, dqp), bt = mul(qb, qa);
+    const f2 qmax = vmax(vmax(vabs(qm1), vabs(qm2)), vmax(vmax(vabs(q0), vabs(qp1)), vabs(qp2)));
+    const f2 rq = rcp(d2qf);
+    f2 rho;
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+        const float a = l ? d2m.y : d2m.x, b = l ? d2c.y : d2c.x, c = l ? d2p.y : d2p.x, d = l ? d2qf.y : d2qf.x;
+        const bool same = (a > 0.0f && b > 0.0f && c > 0.0f && d > 0.0f) || (a < 0.0f && b < 0.0f && c < 0.0f && d < 0.0f);
+        const float mn = minn(minn(l ? cm.y : cm.x, l ? cc.y : cc.x), minn(l ? cp.y : cp.x, fabsf(d)));
+        const float qe = same ? copysignf(mn, d) : 0.0f;
+        const float r = fabsf(d) > 1.0e-12f * (l ? qmax.y : qmax.x) ? qe * (l ? rq.y : rq.x) : 0.0f;
+        if (l) rho.y = r; else rho.x = r;
+    }
+    const f2 tm = fma(mul(S2(-1.0f), rho), dqm, q0), tp = fma(rho, dqp, q0);
+    const f2 t2m = fma(mtwo, dqp, q0), t2p = fma(S2(2.0f), dqm, q0);
+    const f2 adm = vabs(dqm), adp = vabs(dqp);
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+        const bool ext = (l ? at.y : at.x) <= 0.0f || (l ? bt.y : bt.x) <= 0.0f;
+        const bool flat = (l ? rho.y : rho.x) <= 1.0f - 1.0e-12f;
+        const float am = l ? adm.y : adm.x, ap = l ? adp.y : adp.x;
+        const float r0 = l ? dph.y : dph.x, l0 = l ? dphp.y : dphp.x;
+        const float rr = ext ? (flat ? (l ? tm.y : tm.x) : r0) : (am >= 2.0f * ap ? (l ? t2m.y : t2m.x) : r0);
+        const float ll = ext ? (flat ? (l ? tp.y : tp.x) : l0) : (ap >= 2.0f * am ? (l ? t2p.y : t2p.x) : l0);
+        if (l) {
+            qr.y = rr;
+            ql.y = ll;
+        } else {
+            qr.x = rr;
+            ql.x = ll;
+        }
+    }
+}
+
+// Reconstruction of two cells: WENOZ and PPM on the packed pairs; MINMOD
+// (src/fluxlimiter.jl:1-13) runs lane by lane through the scalar FP32 form of
+// vb_physics.cuh, bit-identical to the one-cell-per-thread kernel's.
 template <int REC>
 __device__ __forceinline__ void recon2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& qr, f2& ql) {
     if constexpr (REC == REC_WENOZ) {
         wenoz(qm2, qm1, q0, qp1, qp2, qr, ql);
+    } else if constexpr (REC == REC_PPM) {
+        ppm2(qm2, qm1, q0, qp1, qp2, qr, ql);
     } else {
         recon<REC, float>(qm2.x, qm1.x, q0.x, qp1.x, qp2.x, qr.x, ql.x);
         recon<REC, float>(qm2.y, qm1.y, q0.y, qp1.y, qp2.y, qr.y, ql.y);

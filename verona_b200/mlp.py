@@ -247,7 +247,7 @@ class MLP:
         self.set_params(self.params(), self.norm)
         del torch
 
-    def train(self, n_samples=1 << 22, gammas=(4.0 / 3.0, 5.0 / 3.0), epochs=4, batch=1 << 12, lr=3e-3, seed=0,
+    def train(self, n_samples=1 << 24, gammas=(4.0 / 3.0, 5.0 / 3.0), epochs=4, batch=1 << 12, lr=3e-3, seed=0,
               snapshots=True, log=None):
         """Train on synthetic states (+ solver snapshots); returns the loss history per epoch."""
         import torch
@@ -417,7 +417,7 @@ def main(argv=None):
 
     ap = argparse.ArgumentParser(description="train the learned con2prim guess and save its weights")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
-    ap.add_argument("--samples", type=int, default=1 << 22)
+    ap.add_argument("--samples", type=int, default=1 << 24)
     ap.add_argument("--epochs", type=int, default=4)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--evaluate", action="store_true", help="print the held-out W0 error and Newton iterations")
