@@ -110,7 +110,7 @@ def device_ic(n, seed, noise=0.03):
     return P
 
 
-def make_solver(n, precision, guess, stats=0, c2p_fp32=0):
+def make_solver(n, precision, guess, stats=0, c2p_fp32=1):
     from verona_b200 import Solver
 
     dx = 1.0 / n
@@ -204,13 +204,15 @@ def guess_comparison(n, P0, dt, W, K, dist, learned, stencil_ms_learned, stage_m
     workload, each timed like the headline (stencil and con2prim kernel timed
     apart by the library's profiling events) and run again with iteration
     statistics (W steps, counters reset, 3 steps):
-    - learned_gated: the learned path with the precision gate of the con2prim
-      (options.c2p_fp32: FP32 pressure Newton where the guess has Lorentz
-      factor below sqrt 2 and kinetic energy below 10 x the pressure, FP64
-      for the rest in a second pass);
-    - previous_w: the same W Newton as the learned path, warm-started from the
-      previous state's W instead of the network (the network's contribution
-      alone);
+    - learned (the headline): the network's guess with the precision gate of
+      the con2prim (options.c2p_fp32, the default: FP32 pressure Newton where
+      the guess has Lorentz factor below sqrt 2 and kinetic energy below 10 x
+      the pressure, the FP64 W Newton for the rest in a second pass);
+    - learned_ungated: the same with the FP64 W Newton on every cell;
+    - previous_w: the FP64 W Newton warm-started from the previous state's W
+      instead of the network (the network's contribution alone; ungated, its
+      faster form: the gate in the one-cell-per-thread con2prim kernel runs
+      the FP64 fallback inline and costs time there);
     - previous: the reference's con2prim cascade from the previous state
       (src/3dim/structs.jl:277-287); its counter records the cascade stage that
       converged (1 = the 1DW Newton), not Newton iterations."""
@@ -219,19 +221,20 @@ def guess_comparison(n, P0, dt, W, K, dist, learned, stencil_ms_learned, stage_m
     from verona_b200 import mlp
 
     out = {}
-    arms = (("learned", "learned"), ("learned_gated", "learned"), ("previous_w", "previous_w"),
+    arms = (("learned", "learned"), ("learned_ungated", "learned"), ("previous_w", "previous_w"),
             ("previous", "previous"))
     for name, guess in arms:
         if guess == "learned" and not learned:
             continue
-        gate = int(name == "learned_gated")
+        gate = int(name == "learned")
         if name == "learned":
             out[name] = {"ms_per_step": ms_learned / K, "value": n**3 * K / (ms_learned / 1e3),
                          "stencil_ms_per_stage": stencil_ms_learned,
                          "c2p_ms_per_stage": stage_ms_learned - stencil_ms_learned,
                          "l1_error_vs_fp64": err_learned,
-                         "c2p_kernels": "k_c2p_learned (U from the divergence, network guess, FP64 W Newton "
-                                        "on every cell)"}
+                         "c2p_kernels": "k_c2p_learned (U from the divergence, network guess, FP32 pressure "
+                                        "Newton where the gate admits the cell) + k_c2p_deferred (FP64 W Newton of "
+                                        "the cells the gate leaves)"}
         else:
             s = make_solver(n, "fp32", guess, c2p_fp32=gate)
             if guess == "learned":
@@ -246,9 +249,8 @@ def guess_comparison(n, P0, dt, W, K, dist, learned, stencil_ms_learned, stage_m
                 err = l1_errors(Pa, P64)
                 del Pa
             s.close()
-            kern = {"learned_gated": "k_c2p_learned with the precision gate (FP32 pressure Newton) + k_c2p_deferred "
-                                     "(FP64 W Newton of the cells the gate leaves)",
-                    "previous_w": "k_c2p (the W Newton from the previous state's W)",
+            kern = {"learned_ungated": "k_c2p_learned with the FP64 W Newton on every cell",
+                    "previous_w": "k_c2p (the FP64 W Newton from the previous state's W)",
                     "previous": "k_c2p (the reference cascade from the previous primitive state)"}[name]
             out[name] = {"ms_per_step": ms / K, "value": n**3 * K / (ms / 1e3), "stencil_ms_per_stage": sten,
                          "c2p_ms_per_stage": st_ms / max(st_l, 1) - sten, "l1_error_vs_fp64": err,
@@ -272,7 +274,7 @@ def guess_comparison(n, P0, dt, W, K, dist, learned, stencil_ms_learned, stage_m
             stat["newton_iters_per_cell"] = float(c[2]) / cells
         out[name].update(stat)
     if learned:
-        for base in ("learned_gated", "previous_w", "previous"):
+        for base in ("learned_ungated", "previous_w", "previous"):
             out[f"step_speedup_learned_vs_{base}"] = out[base]["ms_per_step"] / out["learned"]["ms_per_step"]
             out[f"c2p_speedup_learned_vs_{base}"] = out[base]["c2p_ms_per_stage"] / out["learned"]["c2p_ms_per_stage"]
     return out
@@ -647,6 +649,7 @@ def run_ours(args, rank, world, dist):
     achieved = cells * bytes_per_cell_step / 3.0 / (stage_ms_per_launch / 1e3) / 1e9
     form = "_fused" if learned_ok and args.learned_form == "fused" else ""
     form += "_pairs" if args.stencil == "pairs" else ""
+    form += "_gated" if learned_ok else ""  # options.c2p_fp32 = 1, the default
     traffic = read_traffic(f"fp32_{guess}{form}_stage_group")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
@@ -665,7 +668,7 @@ def run_ours(args, rank, world, dist):
                      "traffic": traffic * cells if traffic else None, "peak_kind": peak_kind,
                      "per": "one RK-stage launch of the kernel group over the full grid",
                      "kernel": ("k_stage_zp (z-pair FP32 reconstruct+HLLC+divergence) + k_c2p_learned "
-                                "(RK combination, tensor-core guess, W Newton)" if learned_ok and
+                                "(RK combination, tensor-core guess, gated Newton) + k_c2p_deferred" if learned_ok and
                                 args.learned_form == "fused" else "stencil kernel + con2prim kernel(s)"),
                      "algorithmic_bytes_per_launch": bytes_per_cell_step / 3.0 * cells,
                      "stage_ms_per_launch": stage_ms_per_launch},

@@ -140,7 +140,7 @@ int vb_default_options(vb_options* o) {
     o->floor_ = 1e-7;
     o->w_rtol = 1e-12;
     o->w_max_newton = 8;
-    o->c2p_fp32 = 0;
+    o->c2p_fp32 = 1;
     return VB_OK;
 }
 

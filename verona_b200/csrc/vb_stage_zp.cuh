@@ -4,7 +4,7 @@
 //
 // sm_100a executes FP32 add / multiply / fma on register pairs
 // (FADD2 / FMUL2 / FFMA2: __fadd2_rn, __fmul2_rn, __ffma2_rn), so one
-// instruction advances both cells. Reconstruction (WENOZ), the face floors,
+// instruction advances both cells. Reconstruction (WENOZ, PPM), the face floors,
 // the Riemann flux (HLL / HLLC), the flux difference and its accumulation are
 // written on float2 lanes; reciprocal, square root, min/max and selects stay
 // per lane. Each barrier of the plane loop now serves two planes.
