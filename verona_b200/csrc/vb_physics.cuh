@@ -46,8 +46,9 @@ template <typename T> VB_HD T jsign(T x) { return x > T(0) ? T(1) : (x < T(0) ? 
 // with no branch around it, and the zero's quotient is formed from it:
 //   qdiv:     a * (1 / b), the IEEE quotient of +-0 by any b (signed zero for
 //             a finite nonzero or infinite b, NaN for a zero or NaN b), for
-//             every b except a subnormal below 2^-1024, whose reciprocal
-//             overflows (no divisor of this scheme comes near one);
+//             every b except a subnormal of magnitude at most 2^-1024,
+//             whose reciprocal overflows (no divisor of this scheme comes
+//             near one);
 //   qdiv_pos: a itself, for a b that is positive (or +inf) whenever a is
 //             zero, as the caller's algebra guarantees.
 // Both are bit-identical to the correctly rounded divide on those domains.
