@@ -474,7 +474,16 @@ cudaError_t launch_stage(int dims, int rec, int rs, const StageParams& p, const 
                          cudaStream_t s, int* kernels) {
     *kernels = 1;
     if (dims == 1) return dispatch_stage_dim<1, R>(rec, rs, p, b, s);
-    if (dims == 2) return dispatch_stage_dim<2, R>(rec, rs, p, b, s);
+    if (dims == 2) {
+        if (!p.split || p.skip_c2p) return dispatch_stage_dim<2, R>(rec, rs, p, b, s);
+        // split: the box kernel writes U only, then k_c2p_2d
+        StageParams q = p;
+        q.skip_c2p = 1;
+        const cudaError_t e = dispatch_stage_dim<2, R>(rec, rs, q, b, s);
+        if (e != cudaSuccess) return e;
+        *kernels = 2;
+        return launch_c2p<R>(p, b, s);
+    }
     if (dims == 3) {
         if (zm_fits<R>(p) && !p.force_box) {
             *kernels = p.split && !p.skip_c2p ? 2 : 1;

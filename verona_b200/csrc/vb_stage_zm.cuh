@@ -389,7 +389,64 @@ __global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
 }
 
 // the split con2prim alone (3D interior), e.g. after a kernel that wrote the W guesses
+// The same for a 2D grid (padded extents (Nx + 6, Ny + 6, 1)): one thread per
+// interior cell, the reference's 2D con2prim (solve_cell<2>) from the stage's
+// input P, floors, P out; the statistics as the fused box kernel counts them.
+template <typename R>
+__global__ void __launch_bounds__(256) k_c2p_2d(StageParams p, StageBufs<R> b) {
+    constexpr int NV = 4;
+    const int N0 = p.n[0] - 2 * NG, N1 = p.n[1] - 2 * NG;
+    const long long tot = (long long)N0 * N1;  // < 2^32 (launch_c2p)
+    CellMap cm;
+    cm.init(N0, N1, p.sy, p.sz, NG);
+    unsigned long long n_fail = 0, n_fb = 0, n_it = 0, n_cells = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+         e += (long long)gridDim.x * blockDim.x) {
+        // interior cell (i, j) -> (i + NG) + sy (j + NG); the z index stays 0
+        const uint32_t j = cm.dx.div((uint32_t)e), i = (uint32_t)e - j * cm.n0;
+        const long long c = (long long)(i + NG) + p.sy * (long long)(j + NG);
+        double U[NV], P[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            U[v] = b.Uo[v * p.vs + c];
+            P[v] = (double)b.Pin[v * p.vs + c];
+        }
+        int fb;
+        int r = solve_cell<2>(p, U, P, c, fb);
+        n_fail += (r < 0);
+        n_fb += fb;
+        n_it += (r < 0 ? -r : r);
+        n_cells += 1;
+        P[0] = jmax(P[0], p.floor_);
+        P[1] = jmax(P[1], p.floor_);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) b.Pout[v * p.vs + c] = (R)P[v];
+    }
+    if (n_fail) count_add(p.counters, CNT_C2P_FAIL, n_fail);
+    if (p.stats) {
+        for (int o = 16; o > 0; o >>= 1) {
+            n_fb += __shfl_xor_sync(0xffffffffu, n_fb, o);
+            n_it += __shfl_xor_sync(0xffffffffu, n_it, o);
+            n_cells += __shfl_xor_sync(0xffffffffu, n_cells, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
+            count_add(p.counters, CNT_C2P_ITERS, n_it);
+            count_add(p.counters, CNT_C2P_CELLS, n_cells);
+        }
+    } else if (n_fb) {
+        count_add(p.counters, CNT_C2P_FALLBACK, n_fb);
+    }
+}
+
+// split-mode con2prim of a 3D (k_c2p) or 2D (k_c2p_2d) grid
 template <typename R> cudaError_t launch_c2p(const StageParams& p, const StageBufs<R>& b, cudaStream_t s) {
+    if (p.n[2] == 1) {
+        const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG);
+        if ((unsigned long long)cells > MAX_CELLS_U32) return cudaErrorInvalidValue;
+        k_c2p_2d<R><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
+        return cudaGetLastError();
+    }
     const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
     if ((unsigned long long)cells > MAX_CELLS_U32) return cudaErrorInvalidValue;
     k_c2p<R><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
@@ -438,6 +495,7 @@ template <typename R> int stage_div_in_pout(int dims, int rec, int rs, const Sta
 // launches result from launch_stage with skip_c2p = 1, want_div = 0 followed
 // by launch_c2p
 template <typename R> int stage_split_c2p(int dims, const StageParams& p) {
+    if (dims == 2) return p.split && !p.skip_c2p ? 1 : 0;
     return dims == 3 && !p.force_box && zm_fits<R>(p) && p.split && !p.skip_c2p ? 1 : 0;
 }
 
