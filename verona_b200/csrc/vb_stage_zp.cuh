@@ -4,7 +4,7 @@
 //
 // sm_100a executes FP32 add / multiply / fma on register pairs
 // (FADD2 / FMUL2 / FFMA2: __fadd2_rn, __fmul2_rn, __ffma2_rn), so one
-// instruction advances both cells. Reconstruction (WENOZ, PPM), the face floors,
+// instruction advances both cells. Reconstruction (every limiter), the face floors,
 // the Riemann flux (HLL / HLLC), the flux difference and its accumulation are
 // written on float2 lanes; reciprocal, square root, min/max and selects stay
 // per lane. Each barrier of the plane loop now serves two planes.
@@ -142,10 +142,15 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
 
 // Monotonicity limit of PPM on one lane: the reference's
 // sign(a) == sign(b) == sign(c) ? sign(a) min(C2 |b|, C2 |c|, |a|) : 0, with
-// C2 |b| and C2 |c| already formed (a zero or NaN a gives 0, as there).
+// C2 |b| and C2 |c| already formed. The sign test compares sign bits with
+// integer operations: where one of a, b, c is zero the reference gives 0 and
+// the minimum here is that zero too, so only NaN inputs (a NaN state) differ.
+__device__ __forceinline__ bool same_sign(float a, float b, float c) {
+    const int ia = __float_as_int(a);
+    return ((ia ^ __float_as_int(b)) | (ia ^ __float_as_int(c))) >= 0;
+}
 __device__ __forceinline__ float ppm_mc(float a, float b, float c, float cb, float cc) {
-    const bool same = (a > 0.0f && b > 0.0f && c > 0.0f) || (a < 0.0f && b < 0.0f && c < 0.0f);
-    return same ? copysignf(minn(cb, minn(cc, fabsf(a))), a) : 0.0f;
+    return same_sign(a, b, c) ? copysignf(minn(cb, minn(cc, fabsf(a))), a) : 0.0f;
 }
 
 // PPM (src/fluxlimiter.jl:74-180) on two cells: the interface values, their
@@ -188,7 +193,7 @@ __device__ __forceinline__ void ppm2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& 
 #pragma unroll
     for (int l = 0; l < 2; ++l) {
         const float a = l ? d2m.y : d2m.x, b = l ? d2c.y : d2c.x, c = l ? d2p.y : d2p.x, d = l ? d2qf.y : d2qf.x;
-        const bool same = (a > 0.0f && b > 0.0f && c > 0.0f && d > 0.0f) || (a < 0.0f && b < 0.0f && c < 0.0f && d < 0.0f);
+        const bool same = same_sign(a, b, c) && same_sign(a, d, d);
         const float mn = minn(minn(l ? cm.y : cm.x, l ? cc.y : cc.x), minn(l ? cp.y : cp.x, fabsf(d)));
         const float qe = same ? copysignf(mn, d) : 0.0f;
         const float r = fabsf(d) > 1.0e-12f * (l ? qmax.y : qmax.x) ? qe * (l ? rq.y : rq.x) : 0.0f;
@@ -215,9 +220,21 @@ __device__ __forceinline__ void ppm2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& 
     }
 }
 
-// Reconstruction of two cells: WENOZ and PPM on the packed pairs; MINMOD
-// (src/fluxlimiter.jl:1-13) runs lane by lane through the scalar FP32 form of
-// vb_physics.cuh, bit-identical to the one-cell-per-thread kernel's.
+// MINMOD (src/fluxlimiter.jl:1-13) on two cells: dU = 0.25 (sign(s+) +
+// sign(s-)) min(|s+|, |s-|) is sign(s+) min(...) / 2 where the one-sided
+// slopes share a sign bit and 0 elsewhere (a zero slope makes the minimum
+// zero), so the sign test is one integer comparison per lane.
+__device__ __forceinline__ void minmod2(f2 qm1, f2 q0, f2 qp1, f2& qr, f2& ql) {
+    const f2 sp = sub(qp1, q0), sm = sub(q0, qm1);
+    const f2 m = mul(S2(0.5f), vmin(vabs(sp), vabs(sm)));
+    f2 du;
+    du.x = (__float_as_int(sp.x) ^ __float_as_int(sm.x)) >= 0 ? copysignf(m.x, sp.x) : 0.0f;
+    du.y = (__float_as_int(sp.y) ^ __float_as_int(sm.y)) >= 0 ? copysignf(m.y, sp.y) : 0.0f;
+    qr = sub(q0, du);
+    ql = add(q0, du);
+}
+
+// Reconstruction of two cells on the packed pairs.
 template <int REC>
 __device__ __forceinline__ void recon2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& qr, f2& ql) {
     if constexpr (REC == REC_WENOZ) {
@@ -225,8 +242,7 @@ __device__ __forceinline__ void recon2(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2
     } else if constexpr (REC == REC_PPM) {
         ppm2(qm2, qm1, q0, qp1, qp2, qr, ql);
     } else {
-        recon<REC, float>(qm2.x, qm1.x, q0.x, qp1.x, qp2.x, qr.x, ql.x);
-        recon<REC, float>(qm2.y, qm1.y, q0.y, qp1.y, qp2.y, qr.y, ql.y);
+        minmod2(qm1, q0, qp1, qr, ql);
     }
 }
 
