@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <string.h>
 
 #define VB_HD __host__ __device__ __forceinline__
 
@@ -230,12 +231,87 @@ VB_HD void ppm(T q_im2, T q_im1, T q_i, T q_ip1, T q_ip2, T& qr_out, T& ql_out) 
     ql_out = ql_ip1;
 }
 
-// reconstruction(::Val{M}, ...), src/fluxlimiter.jl:183-200
+// ---- FP32 forms of MINMOD and PPM --------------------------------------------
+// The FP32-bulk kernels test signs by their sign bits with integer operations
+// instead of the reference's three-valued sign(): where an operand is zero
+// the reference's result is 0 and the minimum that the test selects is that
+// zero too, so the values differ only for NaN operands (a NaN state).
+VB_HD int f32_bits(float x) {
+#ifdef __CUDA_ARCH__
+    return __float_as_int(x);
+#else
+    int i;
+    memcpy(&i, &x, 4);
+    return i;
+#endif
+}
+VB_HD bool same_sign3(float a, float b, float c) {
+    const int ia = f32_bits(a);
+    return ((ia ^ f32_bits(b)) | (ia ^ f32_bits(c))) >= 0;
+}
+// NaN-propagating minimum (Julia's min on floats)
+VB_HD float fmin_nan(float a, float b) {
+#ifdef __CUDA_ARCH__
+    float r;
+    asm("min.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+#else
+    return (a != a || b != b) ? a + b : fminf(a, b);
+#endif
+}
+VB_HD void minmod32(float qm1, float q, float qp1, float& qr, float& ql) {
+    const float sp = qp1 - q, sm = q - qm1;
+    const float du = same_sign3(sp, sm, sm) ? copysignf(0.5f * fmin_nan(fabsf(sp), fabsf(sm)), sp) : 0.0f;
+    qr = q - du;
+    ql = q + du;
+}
+VB_HD float ppm_limit32(float a, float b, float c) {  // sign(a) min(1.25|b|, 1.25|c|, |a|) or 0
+    return same_sign3(a, b, c) ? copysignf(fmin_nan(1.25f * fabsf(b), fmin_nan(1.25f * fabsf(c), fabsf(a))), a)
+                               : 0.0f;
+}
+VB_HD void ppm32(float qm2, float qm1, float q, float qp1, float qp2, float& qr_out, float& ql_out) {
+    const float qa = q - qm1, qb = qp1 - q, sm = qm1 + q, sp = q + qp1;
+    float dph = 0.5f * sm + (0.5f / 6.0f) * ((qm1 - qm2) - qb);
+    float dphp = 0.5f * sp + (0.5f / 6.0f) * (qa - (qp2 - qp1));
+    const float d2m = qm2 + q - 2.0f * qm1, d2c = qm1 + qp1 - 2.0f * q, d2p = q + qp2 - 2.0f * qp1;
+    const float qdl = ppm_limit32(3.0f * (sm - 2.0f * dph), d2m, d2c);
+    if ((dph - qm1) * (q - dph) < 0.0f) dph = 0.5f * sm - qdl * (1.0f / 6.0f);
+    const float qdr = ppm_limit32(3.0f * (sp - 2.0f * dphp), d2c, d2p);
+    if ((dphp - q) * (qp1 - dphp) < 0.0f) dphp = 0.5f * sp - qdr * (1.0f / 6.0f);
+    const float d2qf = 6.0f * (dph + dphp - 2.0f * q);
+    const float dqm = q - dph, dqp = dphp - q;
+    const bool same = same_sign3(d2m, d2c, d2p) && same_sign3(d2m, d2qf, d2qf);
+    const float qe =
+        same ? copysignf(fmin_nan(fmin_nan(1.25f * fabsf(d2m), 1.25f * fabsf(d2c)), fmin_nan(1.25f * fabsf(d2p), fabsf(d2qf))),
+                         d2qf)
+             : 0.0f;
+    const float qmax = fmaxf(fmaxf(fabsf(qm1), fabsf(qm2)), fmaxf(fmaxf(fabsf(q), fabsf(qp1)), fabsf(qp2)));
+    const float rho = fabsf(d2qf) > 1.0e-12f * qmax ? qe / d2qf : 0.0f;
+    float qr = dph, ql = dphp;
+    if (dqm * dqp <= 0.0f || qb * qa <= 0.0f) {
+        if (rho <= 1.0f - 1.0e-12f) {
+            qr = q - rho * dqm;
+            ql = q + rho * dqp;
+        }
+    } else {
+        if (fabsf(dqm) >= 2.0f * fabsf(dqp)) qr = q - 2.0f * dqp;
+        if (fabsf(dqp) >= 2.0f * fabsf(dqm)) ql = q + 2.0f * dqm;
+    }
+    qr_out = qr;
+    ql_out = ql;
+}
+
+// reconstruction(::Val{M}, ...), src/fluxlimiter.jl:183-200; the FP32-bulk
+// kernels take the FP32 forms of MINMOD and PPM above
 template <int REC, typename T>
 VB_HD void recon(T q_im2, T q_im1, T q_i, T q_ip1, T q_ip2, T& qr, T& ql) {
-    if (REC == REC_MINMOD)
+    if constexpr (sizeof(T) == 4 && REC == REC_MINMOD)
+        minmod32(q_im1, q_i, q_ip1, qr, ql);
+    else if constexpr (sizeof(T) == 4 && REC == REC_PPM)
+        ppm32(q_im2, q_im1, q_i, q_ip1, q_ip2, qr, ql);
+    else if constexpr (REC == REC_MINMOD)
         minmod(q_im1, q_i, q_ip1, qr, ql);
-    else if (REC == REC_PPM)
+    else if constexpr (REC == REC_PPM)
         ppm(q_im2, q_im1, q_i, q_ip1, q_ip2, qr, ql);
     else
         wenoz(q_im2, q_im1, q_i, q_ip1, q_ip2, qr, ql);
