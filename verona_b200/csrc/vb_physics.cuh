@@ -301,14 +301,62 @@ VB_HD void ppm32(float qm2, float qm1, float q, float qp1, float qp2, float& qr_
     ql_out = ql;
 }
 
+// FP32 WENOZ on the one-sided differences D1..D4 of the five values, which
+// the smoothness indicators and the three stencils share:
+//   beta_k * 12/13 = t_k^2 + (3/13) u_k^2 (t: the second difference, u: the
+//   one-sided combination of each sub-stencil); face value = q_i +
+//   sum_k d_k s_k g_k / sum_k d_k s_k with g_k = f_k - q_i and
+//   s_k = 1 + (tau5 / (beta_k + eps))^2, d = (0.1, 0.6, 0.3).
+// The factor 13/12 cancels in tau5 / beta except against eps (1e-30); the
+// smoothness ratio is capped at 1e9 so that the two faces' denominators
+// (each <= 1e18) share one reciprocal of their product. Same scheme as the
+// reference's WENOZ (src/fluxlimiter.jl:19-71), different FP32 rounding.
+VB_HD float rcp32(float x) {
+#ifdef __CUDA_ARCH__
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+#else
+    return 1.0f / x;
+#endif
+}
+VB_HD void wenoz32(float qm2, float qm1, float q0, float qp1, float qp2, float& qr, float& ql) {
+    const float D1 = qm1 - qm2, D2 = q0 - qm1, D3 = qp1 - q0, D4 = qp2 - qp1;
+    const float r = 3.0f / 13.0f;
+    float t = D2 - D1, u = fmaf(2.0f, D2, t);
+    const float b1 = fmaf(r * u, u, t * t);
+    t = D3 - D2;
+    u = D2 + D3;
+    const float b2 = fmaf(r * u, u, t * t);
+    t = D4 - D3;
+    u = fmaf(-2.0f, D3, t);
+    const float b3 = fmaf(r * u, u, t * t);
+    const float tau = fabsf(b1 - b3);
+    const float i1 = fminf(tau * rcp32(b1 + 1.0e-30f), 1.0e9f);
+    const float i2 = fminf(tau * rcp32(b2 + 1.0e-30f), 1.0e9f);
+    const float i3 = fminf(tau * rcp32(b3 + 1.0e-30f), 1.0e9f);
+    const float s1 = fmaf(i1, i1, 1.0f), s2 = fmaf(i2, i2, 1.0f), s3 = fmaf(i3, i3, 1.0f);
+    const float numl = fmaf(s3, fmaf(1.2f / 6.0f, D3, (-0.3f / 6.0f) * D4),
+                            fmaf(s2, fmaf(1.2f / 6.0f, D3, (0.6f / 6.0f) * D2), s1 * fmaf(0.5f / 6.0f, D2, (-0.2f / 6.0f) * D1)));
+    const float denl = fmaf(0.3f, s3, fmaf(0.6f, s2, 0.1f * s1));
+    const float numr = fmaf(s1, fmaf(-1.2f / 6.0f, D2, (0.3f / 6.0f) * D1),
+                            fmaf(s2, fmaf(-1.2f / 6.0f, D2, (-0.6f / 6.0f) * D3), s3 * fmaf(0.2f / 6.0f, D4, (-0.5f / 6.0f) * D3)));
+    const float denr = fmaf(0.3f, s1, fmaf(0.6f, s2, 0.1f * s3));
+    const float rd = rcp32(denl * denr);
+    ql = fmaf(numl * denr, rd, q0);
+    qr = fmaf(numr * denl, rd, q0);
+}
+
 // reconstruction(::Val{M}, ...), src/fluxlimiter.jl:183-200; the FP32-bulk
-// kernels take the FP32 forms of MINMOD and PPM above
+// kernels take the FP32 forms of MINMOD, PPM and WENOZ above
 template <int REC, typename T>
 VB_HD void recon(T q_im2, T q_im1, T q_i, T q_ip1, T q_ip2, T& qr, T& ql) {
     if constexpr (sizeof(T) == 4 && REC == REC_MINMOD)
         minmod32(q_im1, q_i, q_ip1, qr, ql);
     else if constexpr (sizeof(T) == 4 && REC == REC_PPM)
         ppm32(q_im2, q_im1, q_i, q_ip1, q_ip2, qr, ql);
+    else if constexpr (sizeof(T) == 4)
+        wenoz32(q_im2, q_im1, q_i, q_ip1, q_ip2, qr, ql);
     else if constexpr (REC == REC_MINMOD)
         minmod(q_im1, q_i, q_ip1, qr, ql);
     else if constexpr (REC == REC_PPM)
