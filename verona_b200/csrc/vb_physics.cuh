@@ -6,7 +6,10 @@
 // src/2dim/structs.jl:192,205,212 are fused. The FP64 translation unit is
 // compiled with -fmad=false, so for T = double every result is bit-identical
 // to the reference's rounding (IEEE +,-,*,/,sqrt are correctly rounded on
-// sm_100a). The FP32 unit uses the same code with FP32 constants.
+// sm_100a). The FP32-bulk units use the same code with FP32 constants, except
+// for the reconstructions, which have FP32 forms of their own (minmod32,
+// ppm32, wenoz32: the same schemes with sign-bit tests, shared differences
+// and approximate reciprocals).
 #pragma once
 #include "vb_ns.h"
 #include <cuda_runtime.h>
