@@ -286,38 +286,68 @@ __device__ __forceinline__ void stage_tile(const StageParams& p, const StageBufs
             __syncthreads();
         }
         // 2. reconstruct each cell of the tile (plus one halo cell on each side
-        //    along d) once; store its two face values, floored
+        //    along d) once; store its two face values, floored. The tile's own
+        //    cells go one per thread with every variable; the two halo layers
+        //    then go one (cell, variable) per thread, so that the phase takes
+        //    1 + NV * halo / NT cell reconstructions per thread instead of two
+        //    (with one cell per thread, the halo alone made a second round).
         const int FX = TX + (d == 0), FY = TY + (d == 1), FZ = TZ + (d == 2);
         const int NF = FX * FY * FZ;
-        const int RX = TX + (d == 0 ? 2 : 0), RY = TY + (d == 1 ? 2 : 0), RZ = TZ + (d == 2 ? 2 : 0);
         const int sd = d == 0 ? 1 : (d == 1 ? EX : EX * EY);
         const int vtd = d == 0 ? vt[0] : (d == 1 ? vt[1] : vt[2]);
-        for (int e = tid; e < RX * RY * RZ; e += NT) {
-            int rx = e % RX, ry = (e / RX) % RY, rz = e / (RX * RY);
-            int c[3] = {rx - (d == 0), ry - (d == 1), rz - (d == 2)};
+        // cell c (tile coordinates, c_d in [-1, T_d]): staged base index, its
+        // two faces and whether each is written; false if the cell is unused
+        auto cell_at = [&](int c0, int c1, int c2, int& base, int& fR, int& fL, bool& wR, bool& wL) -> bool {
+            const int c[3] = {c0, c1, c2};
             bool ok = true;
-            #pragma unroll
+#pragma unroll
             for (int a = 0; a < 3; ++a)
                 ok = ok && (a == d ? (c[a] >= -1 && c[a] <= vt[a]) : c[a] < vt[a]);
-            if (!ok) continue;
-            int ex = c[0] + (d == 0 || TMA ? NG : 0), ey = c[1] + (d == 1 || TMA ? NG : 0),
-                ez = c[2] + (d == 2 ? NG : 0);
-            int base = ex + EX * (ey + EY * ez);
-            int fR = c[0] + FX * (c[1] + FY * c[2]);                    // face c_d
-            int fL = fR + (d == 0 ? 1 : (d == 1 ? FX : FX * FY));         // face c_d + 1
+            if (!ok) return false;
+            const int ex = c[0] + (d == 0 || TMA ? NG : 0), ey = c[1] + (d == 1 || TMA ? NG : 0),
+                      ez = c[2] + (d == 2 ? NG : 0);
+            base = ex + EX * (ey + EY * ez);
+            fR = c[0] + FX * (c[1] + FY * c[2]);              // face c_d
+            fL = fR + (d == 0 ? 1 : (d == 1 ? FX : FX * FY));  // face c_d + 1
             const int cd = d == 0 ? c[0] : (d == 1 ? c[1] : c[2]);
-            bool wR = cd >= 0, wL = cd + 1 <= vtd;
+            wR = cd >= 0;
+            wL = cd + 1 <= vtd;
+            return true;
+        };
+        auto recon_var = [&](int v, int base, int fR, int fL, bool wR, bool wL) {
+            const R* q = sP + v * EXT + base;
+            R qr, ql;
+            recon<REC>(q[-2 * sd], q[-sd], q[0], q[sd], q[2 * sd], qr, ql);
+            if (v < 2) {
+                qr = jmax(fl, qr);
+                ql = jmax(fl, ql);
+            }
+            if (wR) sR[v * NF + fR] = qr;
+            if (wL) sL[v * NF + fL] = ql;
+        };
+        for (int e = tid; e < TC; e += NT) {
+            int base, fR, fL;
+            bool wR, wL;
+            if (!cell_at(e % TX, (e / TX) % TY, e / (TX * TY), base, fR, fL, wR, wL)) continue;
 #pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                const R* q = sP + v * EXT + base;
-                R qr, ql;
-                recon<REC>(q[-2 * sd], q[-sd], q[0], q[sd], q[2 * sd], qr, ql);
-                if (v < 2) {
-                    qr = jmax(fl, qr);
-                    ql = jmax(fl, ql);
-                }
-                if (wR) sR[v * NF + fR] = qr;
-                if (wL) sL[v * NF + fL] = ql;
+            for (int v = 0; v < NV; ++v) recon_var(v, base, fR, fL, wR, wL);
+        }
+        {
+            // halo layers c_d = -1 and c_d = T_d: (cell, variable) items, variable-major
+            const int td = d == 0 ? TX : (d == 1 ? TY : TZ);
+            const int HL = TC / td;  // cells per layer
+            for (int e = tid; e < 2 * HL * NV; e += NT) {
+                const int v = e / (2 * HL), h = e - v * 2 * HL, side = h / HL, k = h - side * HL;
+                // k enumerates the layer's cells over the two other axes, x fastest
+                int c[3];
+                const int o0 = d == 0 ? 1 : 0, o1 = d == 2 ? 1 : 2;  // the other axes, in order
+                const int n0 = o0 == 0 ? TX : TY;
+                c[d] = side ? td : -1;
+                c[o0] = k % n0;
+                c[o1] = k / n0;
+                int base, fR, fL;
+                bool wR, wL;
+                if (cell_at(c[0], c[1], c[2], base, fR, fL, wR, wL)) recon_var(v, base, fR, fL, wR, wL);
             }
         }
         __syncthreads();
