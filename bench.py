@@ -408,7 +408,7 @@ def read_traffic(key):
     return None
 
 
-# ---- CPU baseline (the oracle, test infrastructure, as the checker's timing) -------------
+# ---- CPU baseline (the oracle, test infrastructure, timed on the host cores) -----------
 def cpu_baseline(seconds):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import numpy as np

@@ -1,5 +1,5 @@
 """Initial conditions of the reference's jet examples, restated in numpy --
-TEST INFRASTRUCTURE ONLY (the checker of vb_init_prims; the product never
+TEST INFRASTRUCTURE ONLY (vb_init_prims is tested against it; the product never
 imports it).
 
 Follows examples/Jet3D/HARM_jet_breakout.jl:72-118 (3D) and

@@ -4,7 +4,7 @@ Forward and backward of the 4 -> 64 -> 64 -> 64 -> 1 ReLU MLP in FP64 numpy,
 with the parameter layout of include/verona_b200.h (W[in][out]). `bf16=True`
 rounds the tensor-core operands (features, h1, h2, weights) to bfloat16 as the
 GPU does, so the forward can be compared tightly; gradients are compared
-against the plain FP64 backward. This is the checker of the GPU kernels; the
+against the plain FP64 backward. The GPU kernels are tested against it; the
 product never imports it.
 """
 from __future__ import annotations

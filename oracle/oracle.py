@@ -1,7 +1,7 @@
 """ctypes front end of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
-arm import this module, and only as the checker. The product (verona_b200)
+arm import this module, and only to check or time against. The product (verona_b200)
 never imports it.
 
 The oracle is a C FP64 restatement of Wesenheit/Verona's SRHD update

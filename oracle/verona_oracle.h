@@ -4,7 +4,7 @@
  * CPU FP64 restatement of Wesenheit/Verona's SRHD update (Julia), used as the
  * parity oracle for the CUDA path and as the timed CPU baseline. Nothing in the
  * product library links or calls this code; only tests/, __graft_entry__.smoke()
- * and bench.py's cpu_baseline / reference arm do, and only as the checker.
+ * and bench.py's cpu_baseline / reference arm do, and only to check or time against.
  *
  * Parity status: the reference (pure Julia + CUDA.jl) cannot run in this
  * environment, and it ships no tests or golden vectors, so the restatement

@@ -212,8 +212,7 @@ def _jet_problems():
 
 @pytest.mark.parametrize("rk", [2, 3])
 def test_fp64_batch_of_jets_matches_oracle_bitwise(rk):
-    """Jets in the batch (north_star: many Riemann AND jet problems in one
-    launch): per-problem NOZZLE / FIXED-with-decay / OUTFLOW faces, each
+    """Jets in the batch (many Riemann and jet problems in one launch): per-problem NOZZLE / FIXED-with-decay / OUTFLOW faces, each
     problem bit-identical to the oracle's single-grid run with the same
     boundaries, over 9 steps split 4 + 5 (two launches, so the device time that
     switches the decays on carries across launches), and the host times

@@ -1,5 +1,5 @@
 """CPU tests that pin the oracle (the C restatement of the reference) before
-it is trusted as the parity checker of the GPU path.
+it is trusted as the parity reference of the GPU path.
 
 The reference ships no tests or golden vectors and cannot run here (Julia),
 so the pins are: the published exact solution of Marti & Mueller problem 1,
