@@ -168,18 +168,18 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zm(StageParams p, Stage
                 sQL[v * FN + ty * FXR + tx + 1] = ql;
             }
         }
-        for (int e = NT - 1 - tid; e >= 0 && e < 2 * TY; e += NT) {
-            const int r = e >> 1, side = e & 1;
+        // the x halo as (cell, variable) items, on the last threads (the first
+        // ones take the y halo): one variable's reconstruction each instead of
+        // all five on a few threads while the rest wait at the barrier
+        for (int e = NT - 1 - tid; e >= 0 && e < 2 * TY * NV; e += NT) {
+            const int v = e / (2 * TY), rs = e - v * 2 * TY, r = rs >> 1, side = rs & 1;
             const R* q = sPl + (r + 3) * EX + (side ? TX : -1) + 3;
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                R qr, ql;
-                recon_floored<REC>(q + v * PLN, 1, fl, v, qr, ql);
-                if (side)
-                    sQX[v * QXN + r] = qr;
-                else
-                    sQL[v * FN + r * FXR] = ql;
-            }
+            R qr, ql;
+            recon_floored<REC>(q + v * PLN, 1, fl, v, qr, ql);
+            if (side)
+                sQX[v * QXN + r] = qr;
+            else
+                sQL[v * FN + r * FXR] = ql;
         }
         __syncthreads();
         {
@@ -217,18 +217,16 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zm(StageParams p, Stage
                 sQL[v * FN + (ty + 1) * TX + tx] = ql;
             }
         }
-        for (int e = tid; e < 2 * TX; e += NT) {
-            const int cx_ = e % TX, side = e / TX;
+        // the y halo as (cell, variable) items
+        for (int e = tid; e < 2 * TX * NV; e += NT) {
+            const int v = e / (2 * TX), rs = e - v * 2 * TX, cx_ = rs % TX, side = rs / TX;
             const R* q = sPl + ((side ? TY : -1) + 3) * EX + cx_ + 3;
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                R qr, ql;
-                recon_floored<REC>(q + v * PLN, EX, fl, v, qr, ql);
-                if (side)
-                    sQX[v * QXN + cx_] = qr;
-                else
-                    sQL[v * FN + cx_] = ql;
-            }
+            R qr, ql;
+            recon_floored<REC>(q + v * PLN, EX, fl, v, qr, ql);
+            if (side)
+                sQX[v * QXN + cx_] = qr;
+            else
+                sQL[v * FN + cx_] = ql;
         }
         __syncthreads();
         {
