@@ -33,9 +33,10 @@ template <int TX, int TY> struct ZmGeom {
     static constexpr int FXN = (TX + 1) * TY, FYN = TX * (TY + 1);
     static constexpr int FN = FXN > FYN ? FXN : FYN;
     static constexpr int QXN = TX > TY ? TX : TY;
-    static constexpr int ZR = 5;  // z-window ring: planes k-1 .. k+3
+    static constexpr int ZR = 5;        // z-window ring: planes k-1 .. k+3
+    static constexpr int YHN = 2 * TX;  // y-halo face states: ql of row -1, qr of row TY
     template <typename R> static constexpr size_t smem_bytes() {
-        return sizeof(R) * NV * (size_t)(PLN + 2 * FN + QXN + ZR * NT);
+        return sizeof(R) * NV * (size_t)(PLN + 2 * FN + QXN + ZR * NT + YHN);
     }
 };
 
@@ -84,6 +85,8 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zm(StageParams p, Stage
     R* sF = sQL + NV * FN;                      // [NV][FN], face fluxes
     R* sQX = sF + NV * FN;                      // [NV][QXN], right states of the last faces
     R* sZ = sQX + NV * QXN;                     // [ZR][NV][NT], this thread's z-window (private)
+    constexpr int YHN = G::YHN;
+    R* sYH = sZ + G::ZR * NV * NT;              // [NV][YHN], y-halo face states
 
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
@@ -201,6 +204,17 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zm(StageParams p, Stage
 #pragma unroll
             for (int v = 0; v < NV; ++v) sF[v * FN + e * FXR + TX] = F[v];
         }
+        // the y halo as (cell, variable) items, in this phase: it needs only the
+        // staged plane, and it fills the time the last threads spend on the
+        // tile's x-edge faces; its face states go to sYH, since sQL and sQX
+        // still hold the x states here
+        for (int e = tid; e < 2 * TX * NV; e += NT) {
+            const int v = e / (2 * TX), rs = e - v * 2 * TX, cx_ = rs % TX, side = rs / TX;
+            const R* q = sPl + ((side ? TY : -1) + 3) * EX + cx_ + 3;
+            R qr, ql;
+            recon_floored<REC>(q + v * PLN, EX, fl, v, qr, ql);
+            sYH[v * YHN + side * TX + cx_] = side ? qr : ql;
+        }
         __syncthreads();
 #pragma unroll
         for (int v = 0; v < NV; ++v) acc.sub(v, cx, sF[v * FN + ty * FXR + tx + 1], sF[v * FN + ty * FXR + tx]);
@@ -217,22 +231,11 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zm(StageParams p, Stage
                 sQL[v * FN + (ty + 1) * TX + tx] = ql;
             }
         }
-        // the y halo as (cell, variable) items
-        for (int e = tid; e < 2 * TX * NV; e += NT) {
-            const int v = e / (2 * TX), rs = e - v * 2 * TX, cx_ = rs % TX, side = rs / TX;
-            const R* q = sPl + ((side ? TY : -1) + 3) * EX + cx_ + 3;
-            R qr, ql;
-            recon_floored<REC>(q + v * PLN, EX, fl, v, qr, ql);
-            if (side)
-                sQX[v * QXN + cx_] = qr;
-            else
-                sQL[v * FN + cx_] = ql;
-        }
         __syncthreads();
         {
             R PL[NV], F[NV];
 #pragma unroll
-            for (int v = 0; v < NV; ++v) PL[v] = sQL[v * FN + ty * TX + tx];
+            for (int v = 0; v < NV; ++v) PL[v] = ty == 0 ? sYH[v * YHN + tx] : sQL[v * FN + ty * TX + tx];
             face_flux<3, RS>(1, g, PL, qry, F);
 #pragma unroll
             for (int v = 0; v < NV; ++v) sF[v * FN + ty * TX + tx] = F[v];
@@ -242,7 +245,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_stage_zm(StageParams p, Stage
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 PL[v] = sQL[v * FN + TY * TX + e];
-                PR[v] = sQX[v * QXN + e];
+                PR[v] = sYH[v * YHN + TX + e];
             }
             face_flux<3, RS>(1, g, PL, PR, F);
 #pragma unroll
