@@ -36,6 +36,7 @@ sys.path.insert(0, ROOT)
 METRIC = "zone-updates/s on 1 B200, 3D jet: learned+FP32 vs plain FP64 at fixed L1 error"
 UNIT = "zone-updates/s"
 GAMMA = 4.0 / 3.0
+RECON = "wenoz"  # reconstruction of the 3D jet's solvers (--recon; the headline workload is WENOZ)
 
 
 def parse():
@@ -67,6 +68,8 @@ def parse():
     ap.add_argument("--dump", action="store_true",
                     help="also time an asynchronous dump of the interior (vb_dump_begin) overlapped with K steps")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--recon", default="wenoz", choices=["wenoz", "ppm", "minmod"],
+                    help="reconstruction of the 3D jet (the headline workload: wenoz; profiling of the others)")
     ap.add_argument("--workload", default="jet3d", choices=["jet3d", "batch", "jet2d"],
                     help="batch: 256 uneven 1D/2D Riemann problems in one persistent launch (not the headline)")
     return ap.parse_args()
@@ -74,9 +77,9 @@ def parse():
 
 def workload_config(n, guess):
     return {
-        "workload": f"3D relativistic jet {n}^3, WENOZ+HLLC, SSP-RK3, CFL 0.4, gamma 4/3, nozzle r=16 Gamma=10",
+        "workload": f"3D relativistic jet {n}^3, {RECON.upper()}+HLLC, SSP-RK3, CFL 0.4, gamma 4/3, nozzle r=16 Gamma=10",
         "grid": [n, n, n],
-        "recon": "WENOZ",
+        "recon": RECON.upper(),
         "riemann": "HLLC",
         "rk": 3,
         "precision": "fp32 bulk (fp64 U, RK accumulation, con2prim)",
@@ -114,7 +117,7 @@ def make_solver(n, precision, guess, stats=0, c2p_fp32=1):
     from verona_b200 import Solver
 
     dx = 1.0 / n
-    s = Solver(3, (n, n, n), GAMMA, (dx, dx, dx), recon="wenoz", riemann="hllc", rk=3, precision=precision,
+    s = Solver(3, (n, n, n), GAMMA, (dx, dx, dx), recon=RECON, riemann="hllc", rk=3, precision=precision,
                guess=guess, n_iter=50, tol=1e-12, floor=1e-8, stats=stats, c2p_fp32=c2p_fp32)
     s.set_boundary(0, 2, nozzle(n))
     return s
@@ -1014,7 +1017,9 @@ def configs_measure(args, rank, world, dist):
 
 
 def main():
+    global RECON
     args = parse()
+    RECON = args.recon
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
