@@ -813,13 +813,15 @@ def run_batch(args, rank, world, dist):
         print(json.dumps(line), flush=True)
 
 
-def jet2d_measure(n, K, W, rank, world, dist, planes="tma", forms=("fp64", "fp64c", "fp32")):
+def jet2d_measure(n, K, W, rank, world, dist, planes="tma", forms=("fp64", "fp64c", "fp32", "fp32w")):
     """2D relativistic jet n^2, WENOZ + HLLC, SSP-RK3, CFL 0.4, gamma 4/3:
     ambient rho = 1 (3 % seeded noise), p = 1e-3, v = 0; nozzle of radius 32
     cells on the x-lo face (rho 0.01, p 1e-3, Lorentz factor 10 along +x),
     outflow elsewhere. Each form timed over K steps on the device after W:
     fp64 (the plain method, the reference's rounding), fp64c (the plain
-    method with FMA contraction), fp32 (the FP32-bulk form)."""
+    method with FMA contraction), fp32 (the FP32-bulk form with the
+    reference's 2D con2prim), fp32w (the FP32-bulk form with the previous
+    state's W through the gated W Newton, VB_GUESS_PREVIOUS_W)."""
     import math
 
     import torch
@@ -833,9 +835,9 @@ def jet2d_measure(n, K, W, rank, world, dist, planes="tma", forms=("fp64", "fp64
     res = {}
     with Clocks(torch.cuda.current_device()) as clk:
         for form in forms:
-            prec = "fp32" if form == "fp32" else "fp64"
+            prec = "fp32" if form.startswith("fp32") else "fp64"
             s = Solver(2, (n, n), GAMMA, (dx, dx), recon="wenoz", riemann="hllc", rk=3, precision=prec, n_iter=50,
-                       tol=1e-12, floor=1e-8)
+                       tol=1e-12, floor=1e-8, guess="previous_w" if form == "fp32w" else "previous")
             s.set_tuning(tma_tiles=tma, fp64_contract=int(form == "fp64c"))
             tma_active = s.tma_tiles_active
             s.set_boundary(0, 2, [32.0, n / 2, 0.0, 0.01, 1e-3 / (GAMMA - 1), math.sqrt(99.0), 0.0, 0.0])
@@ -875,7 +877,8 @@ def run_jet2d(args, rank, world, dist):
                                "Gamma=10", "grid": [n, n], "tiles": args.planes,
                    "l2": "inputs larger than L2" if n * n * 4 * 8 > 126e6 else "inputs smaller than L2",
                    "parallelism": "replicas"},
-        "fp64": res["fp64"], "fp64_contracted": res["fp64c"], "fp32_bulk": res["fp32"], "clocks": clocks,
+        "fp64": res["fp64"], "fp64_contracted": res["fp64c"], "fp32_bulk": res["fp32"],
+        "fp32_bulk_previous_w": res["fp32w"], "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
 

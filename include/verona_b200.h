@@ -61,8 +61,9 @@ enum { VB_PREC_FP64 = 0, VB_PREC_FP32_BULK = 1 };
 /* con2prim initial guess: the cell's previous primitive state with the
  * reference's con2prim cascade (reference); the learned BF16 MLP guess
  * refined by the W Newton (3D only); or the previous state's W refined by that
- * same W Newton (3D only: the learned path without the network, the baseline
- * of what the network gains) */
+ * same W Newton (2D and 3D: in 3D the learned path without the network, the
+ * baseline of what the network gains; in 2D the state is padded to three
+ * momenta with u^z = 0) */
 enum { VB_GUESS_PREVIOUS = 0, VB_GUESS_LEARNED = 1, VB_GUESS_PREVIOUS_W = 2 };
 /* boundary kinds of vb_set_boundary */
 enum {

@@ -78,6 +78,9 @@ def test_create_rejects_bad_options_without_a_gpu():
                      ({"guess": 1}, _lib.ERR_UNSUPPORTED)):
         o = _lib.default_options(**kw)
         assert L.vb_create(C.byref(h), 2, 8, 8, 1, 3, C.byref(o)) == code, kw
+    # the previous-W guess runs in 2D and 3D, not 1D
+    o = _lib.default_options(guess=2)
+    assert L.vb_create(C.byref(h), 1, 8, 1, 1, 3, C.byref(o)) == _lib.ERR_UNSUPPORTED
     o = _lib.default_options()
     o.version = 99
     assert L.vb_create(C.byref(h), 2, 8, 8, 1, 3, C.byref(o)) == _lib.ERR_ARG

@@ -630,3 +630,40 @@ def test_2d_split_con2prim_matches_fused_bitwise(precision):
     np.testing.assert_array_equal(out[1][0], out[0][0])
     np.testing.assert_array_equal(out[1][1], out[0][1])
     assert list(out[1][2]) == list(out[0][2]) and out[0][2][3] > 0
+
+
+@pytest.mark.parametrize("precision,gate", [("fp64", 0), ("fp32", 0), ("fp32", 1)])
+def test_2d_previous_w_con2prim(oracle, precision, gate):
+    """The previous-W con2prim guess in 2D (VB_GUESS_PREVIOUS_W: the W Newton
+    on the state padded to three momenta, gated to FP32 where options.c2p_fp32
+    admits the cell) against the oracle's reference 2D Newton on the 2D jet:
+    FP64 within the Newton tolerance per field, FP32 bulk within its L1 bar."""
+    from verona_b200 import Solver
+
+    g = 4.0 / 3.0
+    n = (64, 40, 1)
+    P0 = jet_ic(2, n, gamma=g, noise=0.03, seed=27)
+    dxs = [1.0 / 64] * 2
+    dt = 0.4 / sum(1.0 / d for d in dxs)
+    noz = nozzle_params(2, n, 4.0, gamma=g)
+    s = Solver(2, n[:2], g, dxs, recon="wenoz", riemann="hllc", rk=3, precision=precision, guess="previous_w",
+               n_iter=50, tol=1e-12, floor=1e-8, stats=1, c2p_fp32=gate)
+    s.set_boundary(0, 2, noz)
+    s.load_prims(P0)
+    s.step(dt, 8)
+    o = oracle.SolverND(2, n[:2], P0, g, 1e-8, 50, 1e-12, oracle.WENOZ, oracle.HLLC, 3)
+    o.set_grid(*(dxs + [1.0]))
+    o.set_boundary(0, oracle.BC_NOZZLE, noz)
+    o.step(dt, 8)
+    got, ref = s.prims(), o.prims()
+    c = s.counters()
+    assert c[0] == 0 and np.all(np.isfinite(got)) and c[3] > 0
+    if precision == "fp64":
+        e = per_field_rel(got, ref)
+        print("2D previous-W FP64 vs oracle: max rel per field", e, "iterations per cell", c[2] / c[3])
+        assert max(e) < 1e-8
+    else:
+        a, b = got[:, 3:-3, 3:-3], ref[:, 3:-3, 3:-3]
+        l1 = [float(np.mean(np.abs(a[v] - b[v])) / np.mean(np.abs(b[v]))) for v in (0, 1)]
+        print("2D previous-W FP32 gate", gate, "L1 rho, p vs oracle", l1)
+        assert max(l1) < 1e-5

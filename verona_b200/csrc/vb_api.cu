@@ -200,8 +200,10 @@ int vb_create(vb_handle* out, int dims, int nx, int ny, int nz, int nghost, cons
     if (opt.n_iter < 1 || opt.n_iter > 100000) return fail(nullptr, VB_ERR_ARG, "vb_create: n_iter %d", opt.n_iter);
     if (opt.guess < VB_GUESS_PREVIOUS || opt.guess > VB_GUESS_PREVIOUS_W)
         return fail(nullptr, VB_ERR_ARG, "vb_create: guess %d", opt.guess);
-    if (opt.guess != VB_GUESS_PREVIOUS && dims != 3)
-        return fail(nullptr, VB_ERR_UNSUPPORTED, "vb_create: the W-Newton con2prim guesses are provided for 3D grids");
+    if (opt.guess == VB_GUESS_LEARNED && dims != 3)
+        return fail(nullptr, VB_ERR_UNSUPPORTED, "vb_create: the learned con2prim guess is provided for 3D grids");
+    if (opt.guess == VB_GUESS_PREVIOUS_W && dims == 1)
+        return fail(nullptr, VB_ERR_UNSUPPORTED, "vb_create: the previous-W con2prim guess is provided for 2D and 3D grids");
     if (nghost == 0 && (opt.riemann != VB_RIEMANN_HLL || opt.rk != 2 || opt.precision != VB_PREC_FP64))
         return fail(nullptr, VB_ERR_UNSUPPORTED,
                     "vb_create: the 1D reference layout (nghost=0) runs the reference scheme only (HLL, RK2, FP64)");
