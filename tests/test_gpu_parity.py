@@ -368,9 +368,13 @@ def test_2d_tma_tiles_match_loaded_tiles_bitwise(precision, rec, rs):
     """The 2D box-tile stage kernel with its tile (halo on both axes, every
     variable) brought in as one TMA tile, against the same kernel staging
     each axis-extended tile by per-thread loads: the same values reach the
-    same arithmetic, so P and U agree bitwise. 70 x 21 interior cells leave
-    partial tiles on both axes, whose boxes reach past the padded extents
-    (TMA fills zeros there, which no valid cell reads)."""
+    same arithmetic, so in FP64 (built without FMA contraction) P and U agree
+    bitwise. The FP32-bulk units are built with contraction, and the compiler
+    may fuse a multiply-add in one instantiation and not the other, so there
+    the two agree to FP32 rounding (max 1e-7 relative per field measured).
+    70 x 21 interior cells leave partial tiles on both axes, whose boxes reach
+    past the padded extents (TMA fills zeros there, which no valid cell
+    reads)."""
     from verona_b200 import Solver
 
     g = 4.0 / 3.0
@@ -391,8 +395,14 @@ def test_2d_tma_tiles_match_loaded_tiles_bitwise(precision, rec, rs):
         assert c[0] == 0 and c[4] == 0
         out[tma] = (s.prims(), s.cons())
         assert np.all(np.isfinite(out[tma][0]))
-    assert np.array_equal(out[0][0], out[1][0])
-    assert np.array_equal(out[0][1], out[1][1])
+    eP, eU = max(per_field_rel(out[1][0], out[0][0])), max(per_field_rel(out[1][1], out[0][1]))
+    print(precision, rec, rs, "TMA vs loaded: differing P", int(np.sum(out[0][0] != out[1][0])), "max rel P", eP,
+          "U", eU)
+    if precision == "fp64":
+        assert np.array_equal(out[0][0], out[1][0])
+        assert np.array_equal(out[0][1], out[1][1])
+    else:
+        assert eP < 1e-6 and eU < 1e-6
 
 
 def test_diverging_reference_newton_is_counted_as_failure():

@@ -570,6 +570,8 @@ template <typename R> static int step_nd(vb_handle h, double dt, cudaStream_t s)
     p.counters = h->cnt;
     p.force_box = h->tun.force_box;
     p.split = h->tun.split_con2prim < 0 ? default_split(h) : h->tun.split_con2prim;
+    // 2D with the previous-W guess: that con2prim runs only in the split kernel
+    if (h->dims == 2 && h->opt.guess == VB_GUESS_PREVIOUS_W) p.split = 1;
     p.skip_c2p = 0;
     p.pairs = h->tun.fp32_pairs != 0;
     if (h->opt.guess == VB_GUESS_LEARNED) {

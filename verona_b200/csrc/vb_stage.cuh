@@ -119,26 +119,6 @@ __device__ __forceinline__ int solve_cell(const StageParams& p, const double* U,
         fallback = fb;
         return it;
     }
-    if (DIM == 2 && p.c2p_mode == C2P_GUESS_W && !p.w_guess) {
-        // the previous state's W in 2D (VB_GUESS_PREVIOUS_W): the W Newton of
-        // the 3D scheme on the state padded to three momenta (u^z = 0), with
-        // the same precision gate
-        double U5[5] = {U[0], U[1], U[2], U[3], 0.0}, P5[5] = {P[0], P[1], P[2], P[3], 0.0};
-        const double W0 = (P[0] + p.gamma * P[1]) * (sq(P[2]) + sq(P[3]) + 1.0);
-        int it;
-        if (p.c2p_fp32) {
-            int f64 = 1;
-            it = solve_cell_learned(p, U5, P5, (float)W0, &fallback, &f64);
-            if (fp64) *fp64 = f64;
-        } else {
-            int fb;
-            it = c2p_w(p.gamma, U5, W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, P5, &fb);
-            fallback = fb;
-        }
-#pragma unroll
-        for (int v = 0; v < 4; ++v) P[v] = P5[v];
-        return it;
-    }
     if (DIM == 1 || DIM == 2) {
         // The reference's 1D / 2D Newton has no failure signal: a cell that
         // diverges keeps a non-finite state (which then spreads); without

@@ -413,7 +413,26 @@ __global__ void __launch_bounds__(256) k_c2p_2d(StageParams p, StageBufs<R> b) {
             P[v] = (double)b.Pin[v * p.vs + c];
         }
         int fb;
-        int r = solve_cell<2>(p, U, P, c, fb);
+        int r;
+        if (p.c2p_mode == C2P_GUESS_W) {
+            // the previous state's W (VB_GUESS_PREVIOUS_W): the W Newton of the
+            // 3D scheme on the state padded to three momenta (u^z = 0), with
+            // the precision gate of the FP32-bulk form. It runs only here,
+            // where 2D grids with this guess always split their stage, so the
+            // fused box kernels keep their own register allocation.
+            double U5[5] = {U[0], U[1], U[2], U[3], 0.0}, P5[5] = {P[0], P[1], P[2], P[3], 0.0};
+            const double W0 = (P[0] + p.gamma * P[1]) * (sq(P[2]) + sq(P[3]) + 1.0);
+            if (p.c2p_fp32) {
+                int f64;
+                r = c2p_w_gated(p.gamma, U5, (float)W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, true, P5, &fb, &f64);
+            } else {
+                r = c2p_w(p.gamma, U5, W0, p.w_rtol, p.w_max_newton, 4 * p.n_iter, P5, &fb);
+            }
+#pragma unroll
+            for (int v = 0; v < NV; ++v) P[v] = P5[v];
+        } else {
+            r = solve_cell<2>(p, U, P, c, fb);
+        }
         n_fail += (r < 0);
         n_fb += fb;
         n_it += (r < 0 ? -r : r);
