@@ -91,11 +91,13 @@ static __device__ __noinline__ int solve_cell_learned(const StageParams& p, cons
 
 // con2prim of one cell: per-dimension reference algorithm, or the W Newton
 // from a supplied guess with the bracketed fallback.
-template <int DIM>
+// MODE: 0 reads p.c2p_mode at run time; 1 (reference) and 2 (W Newton) fix
+// it at compile time, so a kernel of one mode carries no code of the other.
+template <int DIM, int MODE = 0>
 __device__ __forceinline__ int solve_cell(const StageParams& p, const double* U, double* P, long long gidx,
                                           int& fallback, int* fp64 = nullptr) {
     fallback = 0;
-    if (DIM == 3 && p.c2p_mode == C2P_GUESS_W) {
+    if (DIM == 3 && MODE != 1 && (MODE == 2 || p.c2p_mode == C2P_GUESS_W)) {
         double W0;
         if (p.w_guess) {
             // the learned guess, with the precision gate of the FP32-bulk form

@@ -340,7 +340,7 @@ template <typename R> inline bool zm_fits(const StageParams& p) {
 // Split-mode con2prim: one thread per interior cell, no barriers, no shared
 // memory; reads the stage's U and the guess (the stage's input P, or the
 // per-cell W guesses of p.w_guess), writes the floored P.
-template <typename R>
+template <typename R, int MODE>
 __global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
     constexpr int NV = 5;
     const int N0 = p.n[0] - 2 * NG, N1 = p.n[1] - 2 * NG, N2 = p.n[2] - 2 * NG;
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(256) k_c2p(StageParams p, StageBufs<R> b) {
             P[v] = need_p ? (double)b.Pin[v * p.vs + c] : 0.0;
         }
         int fb, f64 = 1;
-        int r = solve_cell<3>(p, U, P, c, fb, &f64);
+        int r = solve_cell<3, MODE>(p, U, P, c, fb, &f64);
         n_fail += (r < 0);
         n_fb += fb;
         n_it += (r < 0 ? -r : r);
@@ -469,7 +469,10 @@ template <typename R> cudaError_t launch_c2p(const StageParams& p, const StageBu
     }
     const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
     if ((unsigned long long)cells > MAX_CELLS_U32) return cudaErrorInvalidValue;
-    k_c2p<R><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
+    if (p.c2p_mode == C2P_GUESS_W)
+        k_c2p<R, 2><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
+    else
+        k_c2p<R, 1><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
     return cudaGetLastError();
 }
 
@@ -495,7 +498,10 @@ cudaError_t launch_stage_zm_t(const StageParams& p, const StageBufs<R>& b, cudaS
     if (e != cudaSuccess || !SPLIT || p.skip_c2p) return e;
     const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
     if ((unsigned long long)cells > MAX_CELLS_U32) return cudaErrorInvalidValue;
-    k_c2p<R><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
+    if (p.c2p_mode == C2P_GUESS_W)
+        k_c2p<R, 2><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
+    else
+        k_c2p<R, 1><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
     return cudaGetLastError();
 }
 

@@ -853,7 +853,10 @@ cudaError_t launch_stage_zp_t(const StageParams& p, const StageBufs<float>& b, c
     if (e != cudaSuccess || TAIL != ZP_U || p.skip_c2p) return e;
     const long long cells = (long long)(p.n[0] - 2 * NG) * (p.n[1] - 2 * NG) * (p.n[2] - 2 * NG);
     if ((unsigned long long)cells > MAX_CELLS_U32) return cudaErrorInvalidValue;
-    k_c2p<float><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
+    if (p.c2p_mode == C2P_GUESS_W)
+        k_c2p<float, 2><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
+    else
+        k_c2p<float, 1><<<grid_for(cells, 256), 256, 0, s>>>(p, b);
     return cudaGetLastError();
 }
 
