@@ -96,20 +96,21 @@ __device__ __forceinline__ f2 num_scale(f2 num, f2 den_other) { return mul(num, 
 __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2& qr, f2& ql) {
     const f2 D1 = sub(qm1, qm2), D2 = sub(q0, qm1), D3 = sub(qp1, q0), D4 = sub(qp2, qp1);
     const f2 r = S2(3.0f / 13.0f);
+    // beta_k + eps with eps folded into the square term: fma(t, t, eps)
+    const f2 eps = S2(1.0e-30f);
     f2 t = sub(D2, D1);           // q_im2 + q_i - 2 q_im1
     f2 u = fma(S2(2.0f), D2, t);  // q_im2 + 3 q_i - 4 q_im1
-    const f2 b1 = fma(mul(r, u), u, mul(t, t));
+    const f2 b1 = fma(mul(r, u), u, fma(t, t, eps));
     t = sub(D3, D2);  // q_im1 + q_ip1 - 2 q_i
     u = add(D2, D3);  // q_ip1 - q_im1
-    const f2 b2 = fma(mul(r, u), u, mul(t, t));
+    const f2 b2 = fma(mul(r, u), u, fma(t, t, eps));
     t = sub(D4, D3);               // q_ip2 + q_i - 2 q_ip1
     u = fma(S2(-2.0f), D3, t);     // q_ip2 + 3 q_i - 4 q_ip1
-    const f2 b3 = fma(mul(r, u), u, mul(t, t));
-    const f2 eps = S2(1.0e-30f);
+    const f2 b3 = fma(mul(r, u), u, fma(t, t, eps));
     const f2 tau = vabs(sub(b1, b3));
-    f2 i1 = mul(tau, rcp(add(b1, eps)));
-    f2 i2 = mul(tau, rcp(add(b2, eps)));
-    f2 i3 = mul(tau, rcp(add(b3, eps)));
+    f2 i1 = mul(tau, rcp(b1));
+    f2 i2 = mul(tau, rcp(b2));
+    f2 i3 = mul(tau, rcp(b3));
     i1 = P2(fminf(i1.x, 1.0e9f), fminf(i1.y, 1.0e9f));
     i2 = P2(fminf(i2.x, 1.0e9f), fminf(i2.y, 1.0e9f));
     i3 = P2(fminf(i3.x, 1.0e9f), fminf(i3.y, 1.0e9f));
@@ -118,10 +119,12 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
     // right face of cell i (left-biased stencils), weights d_k folded into g_k:
     // 0.1 g1 = 0.1 (5 D2 - 2 D1) / 6, 0.6 g2 = 0.6 (D2 + 2 D3) / 6, 0.3 g3 = 0.3 (4 D3 - D4) / 6
     f2 numl, denl, numr, denr;
+    // (the term 1.2 D3 / 6 of g2 and g3 formed once; on the other face 1.2 D2 / 6)
     {
         const f2 g1 = fma(S2(0.5f / 6.0f), D2, mul(S2(-0.2f / 6.0f), D1));
-        const f2 g2 = fma(S2(1.2f / 6.0f), D3, mul(S2(0.6f / 6.0f), D2));
-        const f2 g3 = fma(S2(1.2f / 6.0f), D3, mul(S2(-0.3f / 6.0f), D4));
+        const f2 m3 = mul(S2(1.2f / 6.0f), D3);
+        const f2 g2 = fma(S2(0.6f / 6.0f), D2, m3);
+        const f2 g3 = fma(S2(-0.3f / 6.0f), D4, m3);
         numl = fma(s3, g3, fma(s2, g2, mul(s1, g1)));
         denl = fma(S2(0.3f), s3, fma(S2(0.6f), s2, mul(S2(0.1f), s1)));
     }
@@ -129,8 +132,9 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
     // 0.1 (2 D4 - 5 D3) / 6, 0.6 (-D3 - 2 D2) / 6, 0.3 (D1 - 4 D2) / 6
     {
         const f2 g1 = fma(S2(0.2f / 6.0f), D4, mul(S2(-0.5f / 6.0f), D3));
-        const f2 g2 = fma(S2(-1.2f / 6.0f), D2, mul(S2(-0.6f / 6.0f), D3));
-        const f2 g3 = fma(S2(-1.2f / 6.0f), D2, mul(S2(0.3f / 6.0f), D1));
+        const f2 m2 = mul(S2(-1.2f / 6.0f), D2);
+        const f2 g2 = fma(S2(-0.6f / 6.0f), D3, m2);
+        const f2 g3 = fma(S2(0.3f / 6.0f), D1, m2);
         numr = fma(s1, g3, fma(s2, g2, mul(s3, g1)));
         denr = fma(S2(0.3f), s1, fma(S2(0.6f), s2, mul(S2(0.1f), s3)));
     }
@@ -305,7 +309,8 @@ __device__ __forceinline__ void face_flux(f2 g, f2 gm1, const f2* PL, const f2* 
     const m2 use_R{lR.x < 0.0f, lR.y < 0.0f};
     const m2 use_L{!use_R.x && lL.x > 0.0f, !use_R.y && lL.y > 0.0f};
     // HLL flux, energy-positive convention: (lR F_L - lL F_R + lR lL (U_R - U_L)) / (lR - lL)
-    const f2 cL = mul(lR, idl), cR = mul(mul(S2(-1.0f), lL), idl), cU = mul(mul(lR, lL), idl);
+    const f2 nlL = mul(S2(-1.0f), lL);
+    const f2 cL = mul(lR, idl), cR = mul(nlL, idl), cU = mul(mul(lR, lL), idl);
     f2 Fh[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) Fh[v] = fma(cU, sub(R.U(v), L.U(v)), fma(cL, L.F(v), mul(cR, R.F(v))));
@@ -318,8 +323,8 @@ __device__ __forceinline__ void face_flux(f2 g, f2 gm1, const f2* PL, const f2* 
         return;
     }
     // star state: E_h, m_h are the HLL state, FE_h, Fm_h the HLL flux
-    const f2 E_h = mul(sub(sub(mul(lR, R.U(1)), mul(lL, L.U(1))), sub(R.F(1), L.F(1))), idl);
-    const f2 m_h = mul(sub(sub(mul(lR, R.U(2 + D)), mul(lL, L.U(2 + D))), sub(R.F(2 + D), L.F(2 + D))), idl);
+    const f2 E_h = mul(sub(fma(lR, R.U(1), mul(nlL, L.U(1))), sub(R.F(1), L.F(1))), idl);
+    const f2 m_h = mul(sub(fma(lR, R.U(2 + D), mul(nlL, L.U(2 + D))), sub(R.F(2 + D), L.F(2 + D))), idl);
     const f2 FE_h = Fh[1], Fm_h = Fh[2 + D];
     const f2 b = add(E_h, Fm_h);
     f2 disc = fma(S2(-4.0f), mul(FE_h, m_h), mul(b, b));
