@@ -328,6 +328,76 @@ def test_fp32_pair_kernel_matches_scalar_kernel(rs, variant, rec):
         assert max(e) < 1e-5
 
 
+def _hllc_star_pressure(g, rho, p, u):
+    """p* of the HLLC star state (Mignone & Bodo 2005) between the 1D states
+    (rho, p, -u) and (rho, p, +u), u the normal four-velocity: the face is
+    left to the HLL flux where p* <= 0."""
+    def side(uu):
+        gam = np.sqrt(1 + uu * uu)
+        v = uu / gam
+        w = rho + g / (g - 1) * p
+        U = np.array([rho * gam, w * gam * gam * v, w * gam * gam - p])
+        F = np.array([rho * gam * v, w * gam * gam * v * v + p, w * gam * gam * v])
+        sig = g * p / w / (gam * gam * (1 - g * p / w))
+        r = np.sqrt(sig * (1 - v * v + sig))
+        return U, F, (v + r) / (1 + sig), (v - r) / (1 + sig)
+
+    UL, FL, lpL, lmL = side(-u)
+    UR, FR, lpR, lmR = side(u)
+    lR, lL = max(lpL, lpR), min(lmL, lmR)
+    Uh = (lR * UR - lL * UL - (FR - FL)) / (lR - lL)
+    Fh = (lR * FL - lL * FR + lR * lL * (UR - UL)) / (lR - lL)
+    b = Uh[2] + Fh[1]
+    ls = 2 * Uh[1] / (b + np.sqrt(max(b * b - 4 * Fh[2] * Uh[1], 0.0)))
+    return Fh[1] - Fh[2] * ls
+
+
+@pytest.mark.parametrize("variant", ["split", "fused"])
+def test_fp32_pair_kernel_hllc_fallback_faces(variant):
+    """Streams that move apart along x and along z (the pair axis): at the
+    two separating planes the HLLC star pressure is negative, so those faces
+    take the HLL flux, the rest the HLLC star flux (lanes of one pair differ
+    where a pair straddles the z plane). The z-pair kernel forms the passive
+    components' HLL flux only where a lane falls back; it must agree with the
+    one-cell-per-thread FP32 kernel to FP32 rounding and stay within the
+    FP32-bulk bar of the FP64 run."""
+    from verona_b200 import Solver
+
+    g = 4.0 / 3.0
+    n = (32, 16, 69)
+    assert _hllc_star_pressure(g, 1.0, 0.1, 0.5) < 0
+    P0 = jet_ic(3, n, gamma=g, noise=0.03, seed=11, p_amb=0.1)
+    P0[2, : 3 + n[0] // 2] = -0.5
+    P0[2, 3 + n[0] // 2 :] = 0.5
+    P0[4, :, :, : 3 + 34] = -0.5
+    P0[4, :, :, 3 + 34 :] = 0.5
+    dxs = [1.0 / 32] * 3
+    dt = 0.4 / sum(1.0 / d for d in dxs)
+    out = {}
+    for name, prec, pairs in (("fp64", "fp64", 0), ("scalar", "fp32", 0), ("pairs", "fp32", 1)):
+        s = Solver(3, n, g, dxs, recon="wenoz", riemann="hllc", rk=3, precision=prec, n_iter=50, tol=1e-12,
+                   floor=1e-8)
+        s.set_tuning(split_con2prim=int(variant == "split"), fp32_pairs=pairs)
+        s.load_prims(P0)
+        s.step(dt, 6)
+        out[name] = s.prims()[:, 3:-3, 3:-3, 3:-3]
+        assert s.counters()[0] == 0
+        assert np.all(np.isfinite(out[name]))
+
+    def l1(a, b, v):
+        return float(np.mean(np.abs(a[v] - b[v])) / np.mean(np.abs(b[v])))
+
+    for v in range(5):
+        d = l1(out["pairs"], out["scalar"], v) if v < 2 else float(
+            np.mean(np.abs(out["pairs"][v] - out["scalar"][v])))
+        print(variant, "var", v, "pairs vs scalar FP32:", d)
+        assert d < 2e-6
+    for name in ("scalar", "pairs"):
+        e = (l1(out[name], out["fp64"], 0), l1(out[name], out["fp64"], 1))
+        print(variant, name, "L1 rho, p vs FP64:", e)
+        assert max(e) < 1e-5
+
+
 @pytest.mark.parametrize("rs", ["hll", "hllc"])
 @pytest.mark.parametrize("variant", ["split", "fused"])
 def test_tma_tiles_match_cp_async_planes_bitwise(rs, variant):

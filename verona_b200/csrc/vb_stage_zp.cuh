@@ -311,9 +311,11 @@ __device__ __forceinline__ void face_flux(f2 g, f2 gm1, const f2* PL, const f2* 
     // HLL flux, energy-positive convention: (lR F_L - lL F_R + lR lL (U_R - U_L)) / (lR - lL)
     const f2 nlL = mul(S2(-1.0f), lL);
     const f2 cL = mul(lR, idl), cR = mul(nlL, idl), cU = mul(mul(lR, lL), idl);
+    auto hll = [&](int v) { return fma(cU, sub(R.U(v), L.U(v)), fma(cL, L.F(v), mul(cR, R.F(v)))); };
     f2 Fh[5];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) Fh[v] = fma(cU, sub(R.U(v), L.U(v)), fma(cL, L.F(v), mul(cR, R.F(v))));
+    for (int v = 0; v < 5; ++v)
+        if (RS == RS_HLL || v == 1 || v == 2 + D) Fh[v] = hll(v);
     if (RS == RS_HLL) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
@@ -342,19 +344,40 @@ __device__ __forceinline__ void face_flux(f2 g, f2 gm1, const f2* PL, const f2* 
     const f2 lkf = mul(lK, sub(fac, S2(1.0f)));  // star flux of a passive component: F + lK (fac - 1) U
     const m2 use_hll{!use_R.x && !use_L.x && (!(ps.x > 0.0f) || !(ls.x >= lL.x && ls.x <= lR.x)),
                      !use_R.y && !use_L.y && (!(ps.y > 0.0f) || !(ls.y >= lL.y && ls.y <= lR.y))};
+    // Passive components (density, transverse momenta): U and F of one side S,
+    // the upwind side of a supersonic face, else the side behind the contact,
+    // selected before the products; a supersonic face gets F_S (lkf -> 0).
+    // Their HLL flux is formed only where a lane falls back to HLL.
+    const m2 sup{use_R.x || use_L.x, use_R.y || use_L.y};
+    const m2 sL{use_L.x || (!use_R.x && left.x), use_L.y || (!use_R.y && left.y)};
+    const f2 gS = sel(sL, L.gam, R.gam), gwS = sel(sL, L.gw, R.gw), uwS = sel(sL, L.uw, R.uw);
+    const f2 unS = sel(sL, L.P[2 + D], R.P[2 + D]);
+    const f2 lkfS = P2(sup.x ? 0.0f : lkf.x, sup.y ? 0.0f : lkf.y);
+    const bool any_hll = use_hll.x || use_hll.y;
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-        const f2 UK = sel(left, L.U(v), R.U(v));
-        const f2 FK = sel(left, L.F(v), R.F(v));
-        f2 fs;
-        if (v == 1)  // E* = (E (lK - vn) + p* ls - p vn) / (lK - ls)
-            fs = fma(lK, sub(mul(fma(UK, dv, sub(mul(ps, ls), mul(p, vn))), ilk), UK), FK);
-        else if (v == 2 + D)  // m* = (m (lK - vn) + p* - p) / (lK - ls)
-            fs = fma(lK, sub(mul(sub(fma(UK, dv, ps), p), ilk), UK), FK);
-        else  // U* = U fac
-            fs = fma(lkf, UK, FK);
-        f2 o = sel(use_R, R.F(v), sel(use_L, L.F(v), sel(use_hll, Fh[v], fs)));
+        f2 o;
+        if (v == 1 || v == 2 + D) {
+            const f2 UK = sel(left, L.U(v), R.U(v));
+            const f2 FK = sel(left, L.F(v), R.F(v));
+            f2 fs;
+            if (v == 1)  // E* = (E (lK - vn) + p* ls - p vn) / (lK - ls)
+                fs = fma(lK, sub(mul(fma(UK, dv, sub(mul(ps, ls), mul(p, vn))), ilk), UK), FK);
+            else  // m* = (m (lK - vn) + p* - p) / (lK - ls)
+                fs = fma(lK, sub(mul(sub(fma(UK, dv, ps), p), ilk), UK), FK);
+            o = sel(use_R, R.F(v), sel(use_L, L.F(v), sel(use_hll, Fh[v], fs)));
+        } else {
+            const f2 PS = sel(sL, L.P[v], R.P[v]);
+            const f2 US = v == 0 ? mul(gS, PS) : mul(PS, gwS);
+            const f2 FS = v == 0 ? mul(PS, unS) : mul(PS, uwS);
+            o = fma(lkfS, US, FS);  // U* = U fac: F + lK (fac - 1) U
+        }
         Fo[v] = v == 1 ? mul(S2(-1.0f), o) : o;
+    }
+    if (any_hll) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v)
+            if (v != 1 && v != 2 + D) Fo[v] = sel(use_hll, hll(v), Fo[v]);
     }
 }
 
