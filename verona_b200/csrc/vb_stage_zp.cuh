@@ -119,6 +119,7 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
     // right face of cell i (left-biased stencils), weights d_k folded into g_k:
     // 0.1 g1 = 0.1 (5 D2 - 2 D1) / 6, 0.6 g2 = 0.6 (D2 + 2 D3) / 6, 0.3 g3 = 0.3 (4 D3 - D4) / 6
     f2 numl, denl, numr, denr;
+    const f2 m6 = mul(S2(0.6f), s2);  // the middle weight's term, common to both denominators
     // (the term 1.2 D3 / 6 of g2 and g3 formed once; on the other face 1.2 D2 / 6)
     {
         const f2 g1 = fma(S2(0.5f / 6.0f), D2, mul(S2(-0.2f / 6.0f), D1));
@@ -126,7 +127,7 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
         const f2 g2 = fma(S2(0.6f / 6.0f), D2, m3);
         const f2 g3 = fma(S2(-0.3f / 6.0f), D4, m3);
         numl = fma(s3, g3, fma(s2, g2, mul(s1, g1)));
-        denl = fma(S2(0.3f), s3, fma(S2(0.6f), s2, mul(S2(0.1f), s1)));
+        denl = fma(S2(0.3f), s3, fma(S2(0.1f), s1, m6));
     }
     // left face of cell i (right-biased stencils), d = (0.1, 0.6, 0.3) on (s3, s2, s1):
     // 0.1 (2 D4 - 5 D3) / 6, 0.6 (-D3 - 2 D2) / 6, 0.3 (D1 - 4 D2) / 6
@@ -136,7 +137,7 @@ __device__ __forceinline__ void wenoz(f2 qm2, f2 qm1, f2 q0, f2 qp1, f2 qp2, f2&
         const f2 g2 = fma(S2(-0.6f / 6.0f), D3, m2);
         const f2 g3 = fma(S2(0.3f / 6.0f), D1, m2);
         numr = fma(s1, g3, fma(s2, g2, mul(s3, g1)));
-        denr = fma(S2(0.3f), s1, fma(S2(0.6f), s2, mul(S2(0.1f), s3)));
+        denr = fma(S2(0.3f), s1, fma(S2(0.1f), s3, m6));
     }
     // 1 / denl = denr / (denl denr), 1 / denr = denl / (denl denr): one reciprocal
     const f2 rd = rcp(mul(denl, denr));
@@ -276,7 +277,7 @@ template <int D> struct Side {
         const f2 igam = mul(wgp, R);
         vn = mul(un, igam);
         const f2 sig = mul(mul(gp, R), igam);
-        const f2 r = vsqrt(mul(sig, add(sub(one, mul(vn, vn)), sig)));
+        const f2 r = vsqrt(mul(sig, sub(sig, fma(vn, vn, S2(-1.0f)))));  // sig (1 - vn^2 + sig)
         const f2 inv = rcp(add(one, sig));
         lp = mul(add(vn, r), inv);
         lm = mul(sub(vn, r), inv);
